@@ -1,0 +1,878 @@
+// C-ABI of libbeampower_b200.so: table management, launch configuration,
+// the stream-ordered device entry points and the host-buffer drop-ins.
+// Declarations and their reference counterparts: include/beampower_b200.h.
+#include <algorithm>
+#include <atomic>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "beampower_b200.h"
+#include "bp_common.cuh"
+#include "bp_kernels.cuh"
+
+namespace {
+
+thread_local std::string g_last_error;
+std::atomic<uint64_t> g_launches{0};
+
+int fail(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return code;
+}
+
+int cuda_fail(cudaError_t e, const char* what) {
+  if (e == cudaErrorMemoryAllocation)
+    return fail(BP_ERR_OUT_OF_MEMORY, "%s: %s", what, cudaGetErrorString(e));
+  return fail(BP_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+#define BP_CUDA(call)                                  \
+  do {                                                 \
+    cudaError_t e_ = (call);                           \
+    if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
+  } while (0)
+
+#define BP_LAUNCHED(what)                                         \
+  do {                                                            \
+    g_launches.fetch_add(1, std::memory_order_relaxed);           \
+    cudaError_t e_ = cudaGetLastError();                          \
+    if (e_ != cudaSuccess) return cuda_fail(e_, "launch " what);   \
+  } while (0)
+
+inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+constexpr long long kMaxInt = std::numeric_limits<int>::max();
+
+// ---- default staged-kernel configuration -----------------------------------
+// 8 consumer warps x 8 sources per thread = 64 sources per tile, 8 samples
+// per lane = 256-sample time tiles, 4-stage ring.
+constexpr int kKS = 8, kMT = 8, kWS = 8, kNStage = 4;
+constexpr int kTileSources = kWS * kKS;
+constexpr int kTimeTile = 32 * kMT;
+static_assert(bp::kMaxTimeTile % kTimeTile == 0, "time tile must divide kMaxTimeTile");
+
+int device_sm_count(int dev) {
+  static int cache[64] = {0};
+  if (dev >= 0 && dev < 64 && cache[dev]) return cache[dev];
+  int v = 0;
+  cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+  if (dev >= 0 && dev < 64) cache[dev] = v;
+  return v;
+}
+
+int device_smem_optin(int dev) {
+  static int cache[64] = {0};
+  if (dev >= 0 && dev < 64 && cache[dev]) return cache[dev];
+  int v = 0;
+  cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  if (dev >= 0 && dev < 64) cache[dev] = v;
+  return v;
+}
+
+}  // namespace
+
+struct bp_table {
+  bp::TableDev dev;
+  bp_table_info info;
+  int32_t* minmax;   // (N, 2) in source order
+  void* mem;         // one device allocation holding everything above
+  void* direct_mem;  // copies of delays / weights when the direct kernel is used
+  int32_t* delays;   // (N, S, P), direct kernel only
+  float* weights;    // (N, S), direct kernel only
+  int* status;       // kernel status word
+  int device;
+  cudaStream_t stream;
+};
+
+namespace {
+
+__global__ void init_stats_kernel(int* stats, int* status) {
+  if (threadIdx.x == 0) {
+    stats[bp::kStatMinDelay] = INT_MAX;
+    stats[bp::kStatMaxDelay] = INT_MIN;
+    stats[bp::kStatMaxSpread] = 0;
+    stats[bp::kStatMaxActive] = 0;
+    stats[bp::kStatNonFinite] = 0;
+    stats[bp::kStatMinLoAligned] = INT_MAX;
+    stats[bp::kStatWideTile] = 0;
+    stats[7] = 0;
+    *status = 0;
+  }
+}
+
+template <int P>
+int launch_table_build(const int32_t* d, const float* w, bp::TableDev& tb, cudaStream_t st) {
+  const size_t smem = (size_t)(2 * tb.S * P + tb.S) * sizeof(int);
+  if (smem > 48 * 1024)
+    BP_CUDA(cudaFuncSetAttribute(bp::table_build_kernel<P>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  bp::table_build_kernel<P><<<tb.n_tiles, 256, smem, st>>>(d, w, tb);
+  BP_LAUNCHED("table_build_kernel");
+  return BP_OK;
+}
+
+size_t pad256(size_t v) { return (v + 255) / 256 * 256; }
+
+// ---- staged kernel dispatch -------------------------------------------------
+template <int P, bool MAXRED, bool CHECKED>
+int launch_window_p(const bp::WindowArgs& a, int dev, cudaStream_t st) {
+  using L = bp::WindowSmem<P, kKS, kMT, kWS, kNStage, MAXRED>;
+  const L lay(a.rowcap, a.max_active);
+  if (lay.total > (size_t)device_smem_optin(dev))
+    return fail(BP_ERR_UNSUPPORTED, "staged kernel needs %zu B of shared memory", lay.total);
+  auto kern = bp::beam_window_kernel<P, kKS, kMT, kWS, kNStage, MAXRED, CHECKED>;
+  BP_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)lay.total));
+  const long long n_chunks = (a.n_tt + a.tiles_per_chunk - 1) / a.tiles_per_chunk;
+  const long long blocks = n_chunks * a.n_tiles;
+  if (blocks > kMaxInt) return fail(BP_ERR_UNSUPPORTED, "grid too large");
+  kern<<<(unsigned)blocks, bp::WindowCfg<P, kKS, kMT, kWS>::kThreads, lay.total, st>>>(a);
+  BP_LAUNCHED("beam_window_kernel");
+  return BP_OK;
+}
+
+template <bool MAXRED, bool CHECKED>
+int launch_window(int P, const bp::WindowArgs& a, int dev, cudaStream_t st) {
+  switch (P) {
+    case 1: return launch_window_p<1, MAXRED, CHECKED>(a, dev, st);
+    case 2: return launch_window_p<2, MAXRED, CHECKED>(a, dev, st);
+    case 3: return launch_window_p<3, MAXRED, CHECKED>(a, dev, st);
+    case 4: return launch_window_p<4, MAXRED, CHECKED>(a, dev, st);
+    default: return fail(BP_ERR_UNSUPPORTED, "staged kernel supports 1..4 phases");
+  }
+}
+
+int staged_smem_bytes(int P, bool maxred, int rowcap, int max_active) {
+  auto f = [&](auto tag) -> size_t {
+    constexpr int PP = decltype(tag)::value;
+    if (maxred) return bp::WindowSmem<PP, kKS, kMT, kWS, kNStage, true>(rowcap, max_active).total;
+    return bp::WindowSmem<PP, kKS, kMT, kWS, kNStage, false>(rowcap, max_active).total;
+  };
+  switch (P) {
+    case 1: return (int)f(std::integral_constant<int, 1>{});
+    case 2: return (int)f(std::integral_constant<int, 2>{});
+    case 3: return (int)f(std::integral_constant<int, 3>{});
+    case 4: return (int)f(std::integral_constant<int, 4>{});
+  }
+  return INT_MAX;
+}
+
+int rowcap_for(const bp_table* t) {
+  return (int)bp::align_up_sz((size_t)(kTimeTile + t->info.max_spread), bp::kAlign);
+}
+
+int choose_tiles_per_chunk(int n_tt, int n_tiles, int dev) {
+  // Enough blocks for load balance (>= ~16 per SM), chunks of at most 64 time
+  // tiles so that the blocks in flight share an L2-resident stretch of trace.
+  const long long want_blocks = 16ll * std::max(1, device_sm_count(dev));
+  long long tpc = (long long)n_tt * n_tiles / std::max(1ll, want_blocks);
+  tpc = std::max(1ll, std::min(tpc, 64ll));
+  return (int)std::min<long long>(tpc, n_tt);
+}
+
+int check_layout(const bp_table* t, size_t n_samples, size_t lpad, size_t pitch) {
+  size_t need_lpad = 0, need_pitch = 0;
+  int rc = bp_trace_layout(t, n_samples, &need_lpad, &need_pitch);
+  if (rc) return rc;
+  if (lpad < need_lpad || pitch < lpad + n_samples ||
+      (t->info.uses_window_kernel && (lpad % bp::kAlign || pitch % bp::kAlign ||
+                                      pitch - lpad < need_pitch - need_lpad)))
+    return fail(BP_ERR_INVALID_ARGUMENT,
+                "trace layout lpad=%zu pitch=%zu too small for this table (need %zu, %zu)", lpad,
+                pitch, need_lpad, need_pitch);
+  return BP_OK;
+}
+
+int run_staged(const bp_table* t, const void* traces, size_t T, size_t lpad, size_t pitch,
+               int out_of_bounds, unsigned long long* keys, float* beam, size_t ldb,
+               cudaStream_t st) {
+  bp::WindowArgs a{};
+  a.traces = reinterpret_cast<const float*>(traces);
+  a.pitch = (long long)pitch;
+  a.lpad = (int)lpad;
+  a.T = (int)T;
+  a.n_tt = (int)((T + kTimeTile - 1) / kTimeTile);
+  a.n_tiles = t->dev.n_tiles;
+  a.tiles_per_chunk = choose_tiles_per_chunk(a.n_tt, a.n_tiles, t->device);
+  a.S = t->dev.S;
+  a.rowcap = rowcap_for(t);
+  a.max_active = std::max(1, t->info.max_active);
+  a.flexible = out_of_bounds;
+  a.src_info = t->dev.src_info;
+  a.tile_hdr = t->dev.tile_hdr;
+  a.st_s = t->dev.st_s;
+  a.st_lo = t->dev.st_lo;
+  a.st_spread = t->dev.st_spread;
+  a.meta = t->dev.meta;
+  a.keys = keys;
+  a.beam = beam;
+  a.ldb = (long long)ldb;
+  a.status = t->status;
+  if (a.n_tt == 0) return BP_OK;
+  const bool checked = out_of_bounds && t->info.any_nonfinite;
+  const bool maxred = keys != nullptr;
+  if (maxred)
+    return checked ? launch_window<true, true>(t->dev.P, a, t->device, st)
+                   : launch_window<true, false>(t->dev.P, a, t->device, st);
+  return checked ? launch_window<false, true>(t->dev.P, a, t->device, st)
+                 : launch_window<false, false>(t->dev.P, a, t->device, st);
+}
+
+int run_direct(const void* traces, int storage, const float* scales, size_t T, size_t lpad,
+               size_t pitch, const int32_t* delays, const float* weights, const int32_t* minmax,
+               size_t N, size_t S, size_t P, int out_of_bounds, unsigned long long* keys,
+               float* beam, size_t ldb, cudaStream_t st) {
+  if (T == 0 || N == 0) return BP_OK;
+  bp::DirectArgs a{};
+  a.traces = traces;
+  a.scales = scales;
+  a.pitch = (long long)pitch;
+  a.lpad = (int)lpad;
+  a.T = (int)T;
+  a.N = (int)N;
+  a.S = (int)S;
+  a.P = (int)P;
+  a.flexible = out_of_bounds;
+  a.src_per_block = 64;
+  a.delays = delays;
+  a.weights = weights;
+  a.minmax = minmax;
+  a.keys = keys;
+  a.beam = beam;
+  a.ldb = (long long)ldb;
+  dim3 grid((unsigned)((T + 255) / 256), (unsigned)((N + a.src_per_block - 1) / a.src_per_block));
+  if (grid.y > 65535) {
+    a.src_per_block = (int)((N + 65534) / 65535);
+    grid.y = (unsigned)((N + a.src_per_block - 1) / a.src_per_block);
+  }
+#define BP_DIRECT(STOR)                                                        \
+  do {                                                                         \
+    if (keys) bp::beam_direct_kernel<STOR, true><<<grid, 256, 0, st>>>(a);     \
+    else bp::beam_direct_kernel<STOR, false><<<grid, 256, 0, st>>>(a);         \
+  } while (0)
+  switch (storage) {
+    case BP_STORAGE_F32: BP_DIRECT(BP_STORAGE_F32); break;
+    case BP_STORAGE_BF16: BP_DIRECT(BP_STORAGE_BF16); break;
+    case BP_STORAGE_F16: BP_DIRECT(BP_STORAGE_F16); break;
+    default: return fail(BP_ERR_INVALID_ARGUMENT, "unknown storage %d", storage);
+  }
+#undef BP_DIRECT
+  BP_LAUNCHED("beam_direct_kernel");
+  return BP_OK;
+}
+
+int check_sizes(size_t T, size_t N, size_t S, size_t P) {
+  if (S == 0 || P == 0) return fail(BP_ERR_INVALID_ARGUMENT, "n_stations and n_phases must be > 0");
+  if (T > (size_t)kMaxInt / 2 || N > (size_t)kMaxInt || S > 65535 || P > 64 ||
+      S * P > 65535)
+    return fail(BP_ERR_UNSUPPORTED, "sizes out of range (T=%zu N=%zu S=%zu P=%zu)", T, N, S, P);
+  return BP_OK;
+}
+
+// Per-thread stream for the host-buffer entry points.
+cudaStream_t host_stream() {
+  thread_local cudaStream_t s = nullptr;
+  thread_local int dev_of_s = -1;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (!s || dev_of_s != dev) {
+    cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+    dev_of_s = dev;
+    // Keep freed stream-ordered allocations in the pool between calls.
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+      uint64_t thr = std::numeric_limits<uint64_t>::max();
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    }
+  }
+  return s;
+}
+
+// Scoped stream-ordered device buffers for the host entry points.
+struct DevBufs {
+  cudaStream_t st;
+  std::vector<void*> ptrs;
+  explicit DevBufs(cudaStream_t s) : st(s) {}
+  template <class T>
+  cudaError_t alloc(T** p, size_t bytes) {
+    void* v = nullptr;
+    cudaError_t e = cudaMallocAsync(&v, std::max<size_t>(bytes, 16), st);
+    if (e == cudaSuccess) ptrs.push_back(v);
+    *p = reinterpret_cast<T*>(v);
+    return e;
+  }
+  ~DevBufs() {
+    for (void* p : ptrs) cudaFreeAsync(p, st);
+    cudaStreamSynchronize(st);
+  }
+};
+
+struct TableGuard {
+  bp_table* t = nullptr;
+  ~TableGuard() {
+    if (t) bp_table_destroy(t);
+  }
+};
+
+int read_status(const bp_table* t, cudaStream_t st) {
+  int status = 0;
+  BP_CUDA(cudaMemcpyAsync(&status, t->status, sizeof(int), cudaMemcpyDeviceToHost, st));
+  BP_CUDA(cudaStreamSynchronize(st));
+  if (status) return fail(BP_ERR_KERNEL, "kernel reported status 0x%x", status);
+  return BP_OK;
+}
+
+void decode_keys_host(const std::vector<unsigned long long>& keys, float* beam_max,
+                      int32_t* argmax) {
+  for (size_t t = 0; t < keys.size(); ++t) {
+    const unsigned long long k = keys[t];
+    if (k) {
+      beam_max[t] = bp::key_value(k);
+      argmax[t] = bp::key_source(k);
+    } else {
+      argmax[t] = 0;
+    }
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* bp_last_error(void) { return g_last_error.c_str(); }
+const char* bp_version(void) { return "beampower_b200 0.1.0 (sm_100a)"; }
+uint64_t bp_launch_count(void) { return g_launches.load(); }
+
+// ---------------------------------------------------------------------------
+// Tables
+// ---------------------------------------------------------------------------
+int bp_table_create(const int32_t* d_delays, const float* d_weights, size_t N, size_t S,
+                    size_t P, void* stream, bp_table** out) {
+  g_last_error.clear();
+  if (!out) return fail(BP_ERR_INVALID_ARGUMENT, "out_table is NULL");
+  *out = nullptr;
+  if (int rc = check_sizes(0, N, S, P)) return rc;
+  if (N > 0 && (!d_delays || !d_weights))
+    return fail(BP_ERR_INVALID_ARGUMENT, "NULL delays or weights");
+  cudaStream_t st = as_stream(stream);
+  bp_table* t = new bp_table();
+  std::memset(t, 0, sizeof(*t));
+  BP_CUDA(cudaGetDevice(&t->device));
+  t->stream = st;
+  const int K = kTileSources;
+  const long long n_tiles = ((long long)N + K - 1) / K;
+  const bool window = P <= 4;
+  const size_t meta_elem = (P <= 2) ? sizeof(uint2) : sizeof(uint4);
+  // one allocation, 256-byte aligned sub-buffers
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    size_t o = off;
+    off += pad256(std::max<size_t>(bytes, 1));
+    return o;
+  };
+  const size_t o_stats = take(bp::kStatCount * sizeof(int));
+  const size_t o_status = take(sizeof(int));
+  const size_t o_minmax = take(N * 2 * sizeof(int32_t));
+  size_t o_src = 0, o_hdr = 0, o_sts = 0, o_stlo = 0, o_stsp = 0, o_meta = 0;
+  if (window && n_tiles > 0) {
+    o_src = take((size_t)n_tiles * K * sizeof(int4));
+    o_hdr = take((size_t)n_tiles * sizeof(int2));
+    o_sts = take((size_t)n_tiles * S * sizeof(int));
+    o_stlo = take((size_t)n_tiles * S * P * sizeof(int));
+    o_stsp = take((size_t)n_tiles * S * P * sizeof(int));
+    o_meta = take((size_t)n_tiles * S * K * meta_elem);
+  }
+  cudaError_t e = cudaMallocAsync(&t->mem, off, st);
+  if (e != cudaSuccess) {
+    delete t;
+    return cuda_fail(e, "cudaMallocAsync(table)");
+  }
+  char* base = reinterpret_cast<char*>(t->mem);
+  t->dev.N = (int)N;
+  t->dev.S = (int)S;
+  t->dev.P = (int)P;
+  t->dev.K = K;
+  t->dev.n_tiles = (int)n_tiles;
+  t->dev.stats = reinterpret_cast<int*>(base + o_stats);
+  t->status = reinterpret_cast<int*>(base + o_status);
+  t->minmax = reinterpret_cast<int32_t*>(base + o_minmax);
+  if (window && n_tiles > 0) {
+    t->dev.src_info = reinterpret_cast<int4*>(base + o_src);
+    t->dev.tile_hdr = reinterpret_cast<int2*>(base + o_hdr);
+    t->dev.st_s = reinterpret_cast<int*>(base + o_sts);
+    t->dev.st_lo = reinterpret_cast<int*>(base + o_stlo);
+    t->dev.st_spread = reinterpret_cast<int*>(base + o_stsp);
+    t->dev.meta = base + o_meta;
+  }
+  t->dev.perm = nullptr;
+
+  auto bail = [&](int rc) {
+    bp_table_destroy(t);
+    return rc;
+  };
+  init_stats_kernel<<<1, 32, 0, st>>>(t->dev.stats, t->status);
+  g_launches.fetch_add(1);
+  if (N > 0) {
+    bp::minmax_kernel<<<(unsigned)((N + 255) / 256), 256, 0, st>>>(d_delays, d_weights, (int)N,
+                                                                  (int)S, (int)P, t->minmax);
+    g_launches.fetch_add(1);
+  }
+  if (cudaError_t le = cudaGetLastError(); le != cudaSuccess)
+    return bail(cuda_fail(le, "launch minmax_kernel"));
+  int rc = BP_OK;
+  if (window && n_tiles > 0) {
+    switch (P) {
+      case 1: rc = launch_table_build<1>(d_delays, d_weights, t->dev, st); break;
+      case 2: rc = launch_table_build<2>(d_delays, d_weights, t->dev, st); break;
+      case 3: rc = launch_table_build<3>(d_delays, d_weights, t->dev, st); break;
+      case 4: rc = launch_table_build<4>(d_delays, d_weights, t->dev, st); break;
+    }
+    if (rc) return bail(rc);
+  }
+  int stats[bp::kStatCount];
+  e = cudaMemcpyAsync(stats, t->dev.stats, sizeof(stats), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return bail(cuda_fail(e, "table statistics"));
+
+  bp_table_info& in = t->info;
+  in.n_sources = (int64_t)N;
+  in.n_stations = (int64_t)S;
+  in.n_phases = (int64_t)P;
+  in.tile_sources = K;
+  in.n_tiles = (int32_t)n_tiles;
+  in.min_delay = stats[bp::kStatMinDelay];
+  in.max_delay = stats[bp::kStatMaxDelay];
+  in.max_spread = stats[bp::kStatMaxSpread];
+  in.max_active = stats[bp::kStatMaxActive];
+  in.any_nonfinite = stats[bp::kStatNonFinite];
+  bool use_window = window && n_tiles > 0 && !stats[bp::kStatWideTile];
+  if (use_window) {
+    const int rowcap = (int)bp::align_up_sz((size_t)(kTimeTile + in.max_spread), bp::kAlign);
+    const int need = staged_smem_bytes((int)P, true, rowcap, std::max(1, in.max_active));
+    if (need > device_smem_optin(t->device)) use_window = false;
+  }
+  in.uses_window_kernel = use_window ? 1 : 0;
+  if (!use_window && N > 0) {
+    // The direct kernel reads the raw arrays: keep private copies.
+    e = cudaMallocAsync(&t->direct_mem, N * S * P * sizeof(int32_t) + N * S * sizeof(float) + 256,
+                        st);
+    if (e != cudaSuccess) return bail(cuda_fail(e, "cudaMallocAsync(table copies)"));
+    t->delays = reinterpret_cast<int32_t*>(t->direct_mem);
+    t->weights = reinterpret_cast<float*>(
+        reinterpret_cast<char*>(t->direct_mem) + pad256(N * S * P * sizeof(int32_t)));
+    e = cudaMemcpyAsync(t->delays, d_delays, N * S * P * sizeof(int32_t),
+                        cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(t->weights, d_weights, N * S * sizeof(float), cudaMemcpyDeviceToDevice,
+                          st);
+    if (e != cudaSuccess) return bail(cuda_fail(e, "copy table arrays"));
+  }
+  *out = t;
+  return BP_OK;
+}
+
+int bp_table_destroy(bp_table* t) {
+  if (!t) return BP_OK;
+  if (t->mem) cudaFreeAsync(t->mem, t->stream);
+  if (t->direct_mem) cudaFreeAsync(t->direct_mem, t->stream);
+  cudaStreamSynchronize(t->stream);
+  delete t;
+  return BP_OK;
+}
+
+int bp_table_get_info(const bp_table* t, bp_table_info* info) {
+  if (!t || !info) return fail(BP_ERR_INVALID_ARGUMENT, "NULL table or info");
+  *info = t->info;
+  return BP_OK;
+}
+
+int bp_trace_layout(const bp_table* t, size_t T, size_t* lpad, size_t* pitch) {
+  if (!t || !lpad || !pitch) return fail(BP_ERR_INVALID_ARGUMENT, "NULL argument");
+  if (!t->info.uses_window_kernel) {  // the direct kernel reads [0, T) only
+    *lpad = 0;
+    *pitch = bp::align_up_sz(std::max<size_t>(T, 1), 64);
+    return BP_OK;
+  }
+  const int mn = t->info.min_delay, mx = t->info.max_delay;
+  const bool any = mn <= mx;
+  // left pad: the lowest aligned window start below zero
+  long long lp = 0;
+  if (any && mn < 0) lp = -(long long)bp::floor_align(mn);
+  lp = (long long)bp::align_up_sz((size_t)lp, 32);
+  const long long right = any ? std::max(0, mx) : 0;
+  const long long p = (long long)bp::align_up_sz(
+      (size_t)(lp + (long long)bp::align_up_sz(T, bp::kMaxTimeTile) + right + 2 * bp::kAlign), 64);
+  *lpad = (size_t)lp;
+  *pitch = (size_t)p;
+  return BP_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Device entry points
+// ---------------------------------------------------------------------------
+int bp_minmax_dev(const int32_t* d, const float* w, size_t N, size_t S, size_t P, int32_t* out,
+                  void* stream) {
+  g_last_error.clear();
+  if (int rc = check_sizes(0, N, S, P)) return rc;
+  if (N == 0) return BP_OK;
+  if (!d || !w || !out) return fail(BP_ERR_INVALID_ARGUMENT, "NULL pointer");
+  bp::minmax_kernel<<<(unsigned)((N + 255) / 256), 256, 0, as_stream(stream)>>>(
+      d, w, (int)N, (int)S, (int)P, out);
+  BP_LAUNCHED("minmax_kernel");
+  return BP_OK;
+}
+
+int bp_prestack_dev(const float* F, const float* alpha, size_t T, size_t S, size_t C, size_t P,
+                    int storage, size_t lpad, size_t pitch, void* traces, float* scales,
+                    void* stream) {
+  g_last_error.clear();
+  if (int rc = check_sizes(T, 0, S, P)) return rc;
+  if (C == 0 || C > 65535) return fail(BP_ERR_INVALID_ARGUMENT, "bad n_channels %zu", C);
+  if (pitch < lpad + T) return fail(BP_ERR_INVALID_ARGUMENT, "pitch < lpad + n_samples");
+  if (!traces || (T > 0 && (!F || !alpha)))
+    return fail(BP_ERR_INVALID_ARGUMENT, "NULL pointer");
+  if (storage != BP_STORAGE_F32)
+    return fail(BP_ERR_UNSUPPORTED, "16-bit storage not built in this version");
+  (void)scales;
+  dim3 grid((unsigned)((pitch + 255) / 256), (unsigned)S);
+  bp::prestack_f32_kernel<<<grid, 256, 0, as_stream(stream)>>>(
+      F, alpha, (int)T, (int)S, (int)C, (int)P, (int)lpad, (long long)pitch,
+      reinterpret_cast<float*>(traces));
+  BP_LAUNCHED("prestack_f32_kernel");
+  return BP_OK;
+}
+
+int bp_traces_from_prestacked_dev(const float* U, size_t T, size_t S, size_t P, size_t lpad,
+                                  size_t pitch, float* traces, void* stream) {
+  g_last_error.clear();
+  if (int rc = check_sizes(T, 0, S, P)) return rc;
+  if (pitch < lpad + T) return fail(BP_ERR_INVALID_ARGUMENT, "pitch < lpad + n_samples");
+  if (!traces || (T > 0 && !U)) return fail(BP_ERR_INVALID_ARGUMENT, "NULL pointer");
+  dim3 grid((unsigned)((pitch + 255) / 256), (unsigned)S);
+  bp::traces_from_prestacked_kernel<<<grid, 256, 0, as_stream(stream)>>>(
+      U, (int)T, (int)S, (int)P, (int)lpad, (long long)pitch, traces);
+  BP_LAUNCHED("traces_from_prestacked_kernel");
+  return BP_OK;
+}
+
+int bp_beamform_max_dev(const bp_table* t, const void* traces, int storage, const float* scales,
+                        size_t T, size_t lpad, size_t pitch, int out_of_bounds,
+                        unsigned long long* keys, float* beam_max, int32_t* argmax,
+                        void* stream) {
+  g_last_error.clear();
+  if (!t) return fail(BP_ERR_INVALID_ARGUMENT, "NULL table");
+  if (out_of_bounds != 0 && out_of_bounds != 1)
+    return fail(BP_ERR_INVALID_ARGUMENT, "out_of_bounds must be 0 or 1");
+  if (int rc = check_sizes(T, t->info.n_sources, t->info.n_stations, t->info.n_phases)) return rc;
+  if (T == 0) return BP_OK;
+  if (!traces || !keys || !beam_max || !argmax)
+    return fail(BP_ERR_INVALID_ARGUMENT, "NULL pointer");
+  if (storage != BP_STORAGE_F32 && !scales)
+    return fail(BP_ERR_INVALID_ARGUMENT, "16-bit storage needs scales");
+  if (int rc = check_layout(t, T, lpad, pitch)) return rc;
+  cudaStream_t st = as_stream(stream);
+  BP_CUDA(cudaMemsetAsync(keys, 0, T * sizeof(unsigned long long), st));
+  int rc;
+  if (t->info.uses_window_kernel && storage == BP_STORAGE_F32) {
+    rc = run_staged(t, traces, T, lpad, pitch, out_of_bounds, keys, nullptr, 0, st);
+  } else if (t->info.uses_window_kernel) {
+    rc = fail(BP_ERR_UNSUPPORTED, "16-bit storage is not built in this version");
+  } else {
+    rc = run_direct(traces, storage, scales, T, lpad, pitch, t->delays, t->weights, t->minmax,
+                    t->info.n_sources, t->info.n_stations, t->info.n_phases, out_of_bounds, keys,
+                    nullptr, 0, st);
+  }
+  if (rc) return rc;
+  bp::decode_keys_kernel<<<(unsigned)((T + 255) / 256), 256, 0, st>>>(keys, (int)T, beam_max,
+                                                                      argmax);
+  BP_LAUNCHED("decode_keys_kernel");
+  return BP_OK;
+}
+
+int bp_beamform_dev(const bp_table* t, const void* traces, int storage, const float* scales,
+                    size_t T, size_t lpad, size_t pitch, int out_of_bounds, float* beam,
+                    size_t ldb, void* stream) {
+  g_last_error.clear();
+  if (!t) return fail(BP_ERR_INVALID_ARGUMENT, "NULL table");
+  if (out_of_bounds != 0 && out_of_bounds != 1)
+    return fail(BP_ERR_INVALID_ARGUMENT, "out_of_bounds must be 0 or 1");
+  if (int rc = check_sizes(T, t->info.n_sources, t->info.n_stations, t->info.n_phases)) return rc;
+  if (T == 0 || t->info.n_sources == 0) return BP_OK;
+  if (!traces || !beam) return fail(BP_ERR_INVALID_ARGUMENT, "NULL pointer");
+  if (ldb < T) return fail(BP_ERR_INVALID_ARGUMENT, "ldb < n_samples");
+  if (storage != BP_STORAGE_F32 && !scales)
+    return fail(BP_ERR_INVALID_ARGUMENT, "16-bit storage needs scales");
+  if (int rc = check_layout(t, T, lpad, pitch)) return rc;
+  if (t->info.uses_window_kernel && storage == BP_STORAGE_F32)
+    return run_staged(t, traces, T, lpad, pitch, out_of_bounds, nullptr, beam, ldb,
+                      as_stream(stream));
+  if (t->info.uses_window_kernel)
+    return fail(BP_ERR_UNSUPPORTED, "16-bit storage is not built in this version");
+  return run_direct(traces, storage, scales, T, lpad, pitch, t->delays, t->weights, t->minmax,
+                    t->info.n_sources, t->info.n_stations, t->info.n_phases, out_of_bounds,
+                    nullptr, beam, ldb, as_stream(stream));
+}
+
+int bp_beamform_max_direct_dev(const void* traces, int storage, const float* scales, size_t T,
+                               size_t lpad, size_t pitch, const int32_t* delays,
+                               const float* weights, size_t N, size_t S, size_t P,
+                               int out_of_bounds, unsigned long long* keys, float* beam_max,
+                               int32_t* argmax, void* stream) {
+  g_last_error.clear();
+  if (int rc = check_sizes(T, N, S, P)) return rc;
+  if (out_of_bounds != 0 && out_of_bounds != 1)
+    return fail(BP_ERR_INVALID_ARGUMENT, "out_of_bounds must be 0 or 1");
+  if (T == 0) return BP_OK;
+  if (!traces || !keys || !beam_max || !argmax || (N > 0 && (!delays || !weights)))
+    return fail(BP_ERR_INVALID_ARGUMENT, "NULL pointer");
+  if (pitch < lpad + T) return fail(BP_ERR_INVALID_ARGUMENT, "pitch < lpad + n_samples");
+  cudaStream_t st = as_stream(stream);
+  BP_CUDA(cudaMemsetAsync(keys, 0, T * sizeof(unsigned long long), st));
+  if (N > 0) {
+    int32_t* mm = nullptr;
+    BP_CUDA(cudaMallocAsync(&mm, N * 2 * sizeof(int32_t), st));
+    bp::minmax_kernel<<<(unsigned)((N + 255) / 256), 256, 0, st>>>(delays, weights, (int)N,
+                                                                  (int)S, (int)P, mm);
+    g_launches.fetch_add(1);
+    int rc = run_direct(traces, storage, scales, T, lpad, pitch, delays, weights, mm, N, S, P,
+                        out_of_bounds, keys, nullptr, 0, st);
+    cudaFreeAsync(mm, st);
+    if (rc) return rc;
+  }
+  bp::decode_keys_kernel<<<(unsigned)((T + 255) / 256), 256, 0, st>>>(keys, (int)T, beam_max,
+                                                                      argmax);
+  BP_LAUNCHED("decode_keys_kernel");
+  return BP_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Host-buffer entry points
+// ---------------------------------------------------------------------------
+namespace {
+
+// Runs the hot path on device buffers already uploaded: table, traces,
+// kernel, and the download of the results.  `traces_fill` writes the trace
+// layout (from prestacked traces or from raw features).
+template <class Fill>
+int host_path(cudaStream_t st, DevBufs& bufs, const int32_t* d_delays, const float* d_w,
+              size_t T, size_t N, size_t S, size_t P, int oob, int reduce, Fill traces_fill,
+              float* beam_max, int32_t* argmax, float* beam) {
+  TableGuard tg;
+  if (int rc = bp_table_create(d_delays, d_w, N, S, P, st, &tg.t)) return rc;
+  size_t lpad = 0, pitch = 0;
+  if (int rc = bp_trace_layout(tg.t, T, &lpad, &pitch)) return rc;
+  float* d_traces = nullptr;
+  BP_CUDA(bufs.alloc(&d_traces, S * P * pitch * sizeof(float)));
+  if (int rc = traces_fill(d_traces, lpad, pitch)) return rc;
+  if (reduce == BP_REDUCE_MAX) {
+    unsigned long long* d_keys = nullptr;
+    float* d_bm = nullptr;
+    int32_t* d_am = nullptr;
+    BP_CUDA(bufs.alloc(&d_keys, T * sizeof(unsigned long long)));
+    BP_CUDA(bufs.alloc(&d_bm, T * sizeof(float)));
+    BP_CUDA(bufs.alloc(&d_am, T * sizeof(int32_t)));
+    if (int rc = bp_beamform_max_dev(tg.t, d_traces, BP_STORAGE_F32, nullptr, T, lpad, pitch, oob,
+                                     d_keys, d_bm, d_am, st))
+      return rc;
+    std::vector<unsigned long long> keys(T);
+    BP_CUDA(cudaMemcpyAsync(keys.data(), d_keys, T * sizeof(unsigned long long),
+                            cudaMemcpyDeviceToHost, st));
+    if (int rc = read_status(tg.t, st)) return rc;
+    decode_keys_host(keys, beam_max, argmax);
+  } else {
+    float* d_beam = nullptr;
+    BP_CUDA(bufs.alloc(&d_beam, std::max<size_t>(N * T, 1) * sizeof(float)));
+    // entries the strict rule leaves alone keep the caller's content
+    BP_CUDA(cudaMemcpyAsync(d_beam, beam, N * T * sizeof(float), cudaMemcpyHostToDevice, st));
+    if (int rc = bp_beamform_dev(tg.t, d_traces, BP_STORAGE_F32, nullptr, T, lpad, pitch, oob,
+                                 d_beam, T, st))
+      return rc;
+    BP_CUDA(cudaMemcpyAsync(beam, d_beam, N * T * sizeof(float), cudaMemcpyDeviceToHost, st));
+    if (int rc = read_status(tg.t, st)) return rc;
+  }
+  return BP_OK;
+}
+
+int prestacked_entry(const float* U, const int* delays, const float* w, size_t T, size_t N,
+                     size_t S, size_t P, int oob, int reduce, float* beam_max, int32_t* argmax,
+                     float* beam) {
+  g_last_error.clear();
+  if (int rc = check_sizes(T, N, S, P)) return rc;
+  if (oob != 0 && oob != 1) return fail(BP_ERR_INVALID_ARGUMENT, "out_of_bounds must be 0 or 1");
+  if (T == 0) return BP_OK;
+  if (!U || (N > 0 && (!delays || !w)))
+    return fail(BP_ERR_INVALID_ARGUMENT, "NULL input pointer");
+  if (reduce == BP_REDUCE_MAX && (!beam_max || !argmax))
+    return fail(BP_ERR_INVALID_ARGUMENT, "NULL output pointer");
+  if (reduce == BP_REDUCE_NONE && N > 0 && !beam)
+    return fail(BP_ERR_INVALID_ARGUMENT, "NULL output pointer");
+  if (N == 0) {
+    if (reduce == BP_REDUCE_MAX) std::fill(argmax, argmax + T, 0);
+    return BP_OK;
+  }
+  cudaStream_t st = host_stream();
+  DevBufs bufs(st);
+  float* d_U = nullptr;
+  int32_t* d_d = nullptr;
+  float* d_w = nullptr;
+  BP_CUDA(bufs.alloc(&d_U, S * T * P * sizeof(float)));
+  BP_CUDA(bufs.alloc(&d_d, N * S * P * sizeof(int32_t)));
+  BP_CUDA(bufs.alloc(&d_w, N * S * sizeof(float)));
+  BP_CUDA(cudaMemcpyAsync(d_U, U, S * T * P * sizeof(float), cudaMemcpyHostToDevice, st));
+  BP_CUDA(cudaMemcpyAsync(d_d, delays, N * S * P * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+  BP_CUDA(cudaMemcpyAsync(d_w, w, N * S * sizeof(float), cudaMemcpyHostToDevice, st));
+  auto fill = [&](float* d_traces, size_t lpad, size_t pitch) {
+    return bp_traces_from_prestacked_dev(d_U, T, S, P, lpad, pitch, d_traces, st);
+  };
+  return host_path(st, bufs, d_d, d_w, T, N, S, P, oob, reduce, fill, beam_max, argmax, beam);
+}
+
+}  // namespace
+
+extern "C" {
+
+int beamform(float* waveform_features, int* time_delays, float* weights, size_t n_samples,
+             size_t n_sources, size_t n_stations, size_t n_phases, int out_of_bounds,
+             float* beam) {
+  return prestacked_entry(waveform_features, time_delays, weights, n_samples, n_sources,
+                          n_stations, n_phases, out_of_bounds, BP_REDUCE_NONE, nullptr, nullptr,
+                          beam);
+}
+
+int beamform_max(float* waveform_features, int* time_delays, float* weights, size_t n_samples,
+                 size_t n_sources, size_t n_stations, size_t n_phases, int out_of_bounds,
+                 float* beam_max, int* source_index_beam_max) {
+  return prestacked_entry(waveform_features, time_delays, weights, n_samples, n_sources,
+                          n_stations, n_phases, out_of_bounds, BP_REDUCE_MAX, beam_max,
+                          source_index_beam_max, nullptr);
+}
+
+int prestack_waveform_features(float* F, float* alpha, size_t T, size_t S, size_t C, size_t P,
+                               int num_threads, float* out) {
+  (void)num_threads;
+  g_last_error.clear();
+  if (int rc = check_sizes(T, 0, S, P)) return rc;
+  if (C == 0 || C > 65535) return fail(BP_ERR_INVALID_ARGUMENT, "bad n_channels %zu", C);
+  if (T == 0) return BP_OK;
+  if (!F || !alpha || !out) return fail(BP_ERR_INVALID_ARGUMENT, "NULL pointer");
+  cudaStream_t st = host_stream();
+  DevBufs bufs(st);
+  float *d_F = nullptr, *d_a = nullptr, *d_rows = nullptr, *d_U = nullptr;
+  BP_CUDA(bufs.alloc(&d_F, S * C * T * sizeof(float)));
+  BP_CUDA(bufs.alloc(&d_a, S * C * P * sizeof(float)));
+  BP_CUDA(bufs.alloc(&d_rows, S * P * T * sizeof(float)));
+  BP_CUDA(bufs.alloc(&d_U, S * T * P * sizeof(float)));
+  BP_CUDA(cudaMemcpyAsync(d_F, F, S * C * T * sizeof(float), cudaMemcpyHostToDevice, st));
+  BP_CUDA(cudaMemcpyAsync(d_a, alpha, S * C * P * sizeof(float), cudaMemcpyHostToDevice, st));
+  if (int rc = bp_prestack_dev(d_F, d_a, T, S, C, P, BP_STORAGE_F32, 0, T, d_rows, nullptr, st))
+    return rc;
+  // rows (S, P, T) -> (S, T, P), the reference's prestack layout
+  dim3 grid((unsigned)((T + 255) / 256), (unsigned)S);
+  bp::rows_to_prestacked_kernel<<<grid, 256, 0, st>>>(d_rows, (int)T, (int)S, (int)P, d_U);
+  BP_LAUNCHED("rows_to_prestacked_kernel");
+  BP_CUDA(cudaMemcpyAsync(out, d_U, S * T * P * sizeof(float), cudaMemcpyDeviceToHost, st));
+  BP_CUDA(cudaStreamSynchronize(st));
+  return BP_OK;
+}
+
+int bp_beamform_host(const float* F, const float* alpha, const int32_t* delays, const float* w,
+                     size_t T, size_t N, size_t S, size_t C, size_t P, int oob, int reduce,
+                     int storage, float* beam_max, int32_t* argmax, float* beam) {
+  g_last_error.clear();
+  if (int rc = check_sizes(T, N, S, P)) return rc;
+  if (C == 0 || C > 65535) return fail(BP_ERR_INVALID_ARGUMENT, "bad n_channels %zu", C);
+  if (oob != 0 && oob != 1) return fail(BP_ERR_INVALID_ARGUMENT, "out_of_bounds must be 0 or 1");
+  if (reduce != BP_REDUCE_MAX && reduce != BP_REDUCE_NONE)
+    return fail(BP_ERR_INVALID_ARGUMENT, "reduce must be BP_REDUCE_MAX or BP_REDUCE_NONE");
+  if (storage != BP_STORAGE_F32)
+    return fail(BP_ERR_UNSUPPORTED, "16-bit storage is not built in this version");
+  if (T == 0) return BP_OK;
+  if (!F || !alpha || (N > 0 && (!delays || !w)))
+    return fail(BP_ERR_INVALID_ARGUMENT, "NULL input pointer");
+  if (reduce == BP_REDUCE_MAX && (!beam_max || !argmax))
+    return fail(BP_ERR_INVALID_ARGUMENT, "NULL output pointer");
+  if (reduce == BP_REDUCE_NONE && N > 0 && !beam)
+    return fail(BP_ERR_INVALID_ARGUMENT, "NULL output pointer");
+  if (N == 0) {
+    if (reduce == BP_REDUCE_MAX) std::fill(argmax, argmax + T, 0);
+    return BP_OK;
+  }
+  cudaStream_t st = host_stream();
+  DevBufs bufs(st);
+  float *d_F = nullptr, *d_a = nullptr, *d_w = nullptr;
+  int32_t* d_d = nullptr;
+  BP_CUDA(bufs.alloc(&d_d, N * S * P * sizeof(int32_t)));
+  BP_CUDA(bufs.alloc(&d_w, N * S * sizeof(float)));
+  BP_CUDA(bufs.alloc(&d_F, S * C * T * sizeof(float)));
+  BP_CUDA(bufs.alloc(&d_a, S * C * P * sizeof(float)));
+  BP_CUDA(cudaMemcpyAsync(d_d, delays, N * S * P * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+  BP_CUDA(cudaMemcpyAsync(d_w, w, N * S * sizeof(float), cudaMemcpyHostToDevice, st));
+  BP_CUDA(cudaMemcpyAsync(d_F, F, S * C * T * sizeof(float), cudaMemcpyHostToDevice, st));
+  BP_CUDA(cudaMemcpyAsync(d_a, alpha, S * C * P * sizeof(float), cudaMemcpyHostToDevice, st));
+  auto fill = [&](float* d_traces, size_t lpad, size_t pitch) {
+    return bp_prestack_dev(d_F, d_a, T, S, C, P, BP_STORAGE_F32, lpad, pitch, d_traces, nullptr,
+                           st);
+  };
+  return host_path(st, bufs, d_d, d_w, T, N, S, P, oob, reduce, fill, beam_max, argmax, beam);
+}
+
+}  // extern "C"
+
+extern "C" {
+
+int bp_beamform_differential_dev(const float* traces, size_t T, size_t lpad, size_t pitch,
+                                 const int32_t* delays, const float* weights, size_t N, size_t S,
+                                 size_t P, float* beam, void* stream) {
+  g_last_error.clear();
+  if (int rc = check_sizes(T, N, S, P)) return rc;
+  if (N == 0 || T == 0) return BP_OK;
+  if (!traces || !delays || !weights || !beam) return fail(BP_ERR_INVALID_ARGUMENT, "NULL pointer");
+  if (pitch < lpad + T) return fail(BP_ERR_INVALID_ARGUMENT, "pitch < lpad + n_samples");
+  bp::differential_kernel<<<(unsigned)((N + 127) / 128), 128, 0, as_stream(stream)>>>(
+      traces, (long long)pitch, (int)lpad, (int)T, delays, weights, (int)N, (int)S, (int)P, beam);
+  BP_LAUNCHED("differential_kernel");
+  return BP_OK;
+}
+
+int beamform_differential(float* U, int* delays, float* w, size_t T, size_t N, size_t S,
+                          size_t P, int num_threads, float* beam) {
+  (void)num_threads;
+  g_last_error.clear();
+  if (int rc = check_sizes(T, N, S, P)) return rc;
+  if (N == 0 || T == 0) return BP_OK;
+  if (!U || !delays || !w || !beam) return fail(BP_ERR_INVALID_ARGUMENT, "NULL pointer");
+  cudaStream_t st = host_stream();
+  DevBufs bufs(st);
+  float *d_U = nullptr, *d_rows = nullptr, *d_w = nullptr, *d_beam = nullptr;
+  int32_t* d_d = nullptr;
+  BP_CUDA(bufs.alloc(&d_U, S * T * P * sizeof(float)));
+  BP_CUDA(bufs.alloc(&d_rows, S * P * T * sizeof(float)));
+  BP_CUDA(bufs.alloc(&d_d, N * S * P * sizeof(int32_t)));
+  BP_CUDA(bufs.alloc(&d_w, N * S * sizeof(float)));
+  BP_CUDA(bufs.alloc(&d_beam, N * sizeof(float)));
+  BP_CUDA(cudaMemcpyAsync(d_U, U, S * T * P * sizeof(float), cudaMemcpyHostToDevice, st));
+  BP_CUDA(cudaMemcpyAsync(d_d, delays, N * S * P * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+  BP_CUDA(cudaMemcpyAsync(d_w, w, N * S * sizeof(float), cudaMemcpyHostToDevice, st));
+  BP_CUDA(cudaMemcpyAsync(d_beam, beam, N * sizeof(float), cudaMemcpyHostToDevice, st));
+  if (int rc = bp_traces_from_prestacked_dev(d_U, T, S, P, 0, T, d_rows, st)) return rc;
+  if (int rc = bp_beamform_differential_dev(d_rows, T, 0, T, d_d, d_w, N, S, P, d_beam, st))
+    return rc;
+  BP_CUDA(cudaMemcpyAsync(beam, d_beam, N * sizeof(float), cudaMemcpyDeviceToHost, st));
+  BP_CUDA(cudaStreamSynchronize(st));
+  return BP_OK;
+}
+
+}  // extern "C"

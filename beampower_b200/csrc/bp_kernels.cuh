@@ -1,0 +1,671 @@
+// sm_100a kernels of the beamforming hot path.
+//
+// Data layout in HBM
+//   traces   row r = s * P + p holds phase p of station s: element (s, p, t)
+//            at traces[r * pitch + lpad + t]; indexes outside [lpad, lpad + T)
+//            are zero.  Written once per record by the prestack kernel.
+//   table    built once per (time_delays, weights) pair: sources grouped in
+//            tiles of K; per tile the active stations (some source of the
+//            tile weights them), per (tile, station, phase) the delay window
+//            lo .. lo + spread (lo aligned down to kAlign samples), per
+//            (tile, station, source) the weight and the delay offsets
+//            d - lo as 16-bit integers, per source its min/max delay over
+//            weighted stations (the strict validity rule).
+//   keys     (T,) uint64 packed (beam, source) keys, max-reduced in place.
+#pragma once
+
+#include <cfloat>
+#include <climits>
+#include <cstdint>
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include "bp_common.cuh"
+
+namespace bp {
+
+// Window starts are aligned down to this many samples (32 bytes of FP32,
+// 16 bytes of 16-bit storage), so every bulk copy starts 16-byte aligned.
+constexpr int kAlign = 8;
+// Largest time tile of any kernel configuration; trace layouts are padded
+// for it so that one layout serves every configuration.
+constexpr int kMaxTimeTile = 1024;
+
+// ---------------------------------------------------------------------------
+// Table (device view)
+// ---------------------------------------------------------------------------
+struct TableDev {
+  int N, S, P, K, n_tiles;
+  int4* src_info;    // [n_tiles * K]  {source index or -1, min delay, max delay, 0}
+  int2* tile_hdr;    // [n_tiles]      {active stations, 0}
+  int* st_s;         // [n_tiles * S]  station of active slot j
+  int* st_lo;        // [n_tiles * S * P] window start (aligned)
+  int* st_spread;    // [n_tiles * S * P] window span beyond the time tile
+  void* meta;        // [n_tiles * S * K] MetaT<P>
+  int* stats;        // [kStatCount]
+  const int* perm;   // optional [n_tiles * K] source order (nullptr: identity)
+};
+
+enum : int {
+  kStatMinDelay = 0,   // min delay over weighted terms
+  kStatMaxDelay = 1,   // max delay over weighted terms
+  kStatMaxSpread = 2,  // max window span (hi - lo_aligned)
+  kStatMaxActive = 3,  // max active stations in a tile
+  kStatNonFinite = 4,  // a non-zero weight is NaN or inf
+  kStatMinLoAligned = 5,
+  kStatWideTile = 6,   // a window span does not fit 16-bit offsets
+  kStatCount = 8
+};
+
+// Per (tile, station, source) metadata: weight bits and 16-bit offsets.
+template <int P> struct MetaT;
+template <> struct MetaT<1> { using type = uint2; };  // {w, off0}
+template <> struct MetaT<2> { using type = uint2; };  // {w, off0 | off1 << 16}
+template <> struct MetaT<3> { using type = uint4; };  // {w, off0|off1<<16, off2, 0}
+template <> struct MetaT<4> { using type = uint4; };  // {w, off0|off1<<16, off2|off3<<16, 0}
+
+template <int P>
+__host__ __device__ __forceinline__ int meta_off(const typename MetaT<P>::type& m, int p) {
+  if constexpr (P <= 2) {
+    return (p == 0) ? (int)(m.y & 0xFFFFu) : (int)(m.y >> 16);
+  } else {
+    const uint32_t v = (p < 2) ? m.y : m.z;
+    return (p & 1) ? (int)(v >> 16) : (int)(v & 0xFFFFu);
+  }
+}
+
+__host__ __device__ __forceinline__ int floor_align(int v) {
+  return (v >= 0) ? (v / kAlign) * kAlign : -(((-v) + kAlign - 1) / kAlign) * kAlign;
+}
+
+// ---------------------------------------------------------------------------
+// Table build: one block per source tile.
+// Dynamic shared memory: 2 * S * P ints (per-station lo / hi) + S ints.
+// ---------------------------------------------------------------------------
+template <int P>
+__global__ void table_build_kernel(const int32_t* __restrict__ delays,
+                                   const float* __restrict__ weights, TableDev tb) {
+  using M = typename MetaT<P>::type;
+  extern __shared__ int sh[];
+  const int S = tb.S, K = tb.K;
+  int* lo = sh;               // [S * P]
+  int* hi = lo + S * P;       // [S * P]
+  int* slot = hi + S * P;     // [S] active slot of station s, or -1
+  __shared__ int n_active_sh;
+  const int tile = blockIdx.x;
+
+  auto orig_of = [&](int k) -> int {
+    const long long idx = (long long)tile * K + k;
+    int o = tb.perm ? tb.perm[idx] : (int)idx;
+    return (o >= 0 && o < tb.N) ? o : -1;
+  };
+
+  // 1. per source: min / max over weighted stations, non-finite weights.
+  for (int k = threadIdx.x; k < K; k += blockDim.x) {
+    const int o = orig_of(k);
+    int mn = INT_MAX, mx = INT_MIN, bad = 0;
+    if (o >= 0) {
+      const int32_t* d = delays + (size_t)o * S * P;
+      const float* w = weights + (size_t)o * S;
+      for (int s = 0; s < S; ++s) {
+        const float ws = w[s];
+        if (ws == 0.0f) continue;
+        if (!isfinite(ws)) bad = 1;
+        for (int p = 0; p < P; ++p) {
+          const int v = d[s * P + p];
+          mn = min(mn, v);
+          mx = max(mx, v);
+        }
+      }
+    }
+    tb.src_info[(size_t)tile * K + k] = make_int4(o, mn, mx, 0);
+    if (bad) atomicOr(&tb.stats[kStatNonFinite], 1);
+  }
+  // 2. per (station, phase): window over the tile's weighted sources.
+  for (int sp = threadIdx.x; sp < S * P; sp += blockDim.x) {
+    const int s = sp / P;
+    int l = INT_MAX, h = INT_MIN;
+    for (int k = 0; k < K; ++k) {
+      const int o = orig_of(k);
+      if (o < 0) continue;
+      if (weights[(size_t)o * S + s] == 0.0f) continue;
+      const int v = delays[(size_t)o * S * P + sp];
+      l = min(l, v);
+      h = max(h, v);
+    }
+    lo[sp] = l;
+    hi[sp] = h;
+  }
+  __syncthreads();
+  // 3. active station list, ascending station index (the summation order).
+  if (threadIdx.x == 0) {
+    int n = 0, spread_max = 0, mn = INT_MAX, mx = INT_MIN, lo_al_min = INT_MAX, wide = 0;
+    for (int s = 0; s < S; ++s) {
+      if (lo[s * P] > hi[s * P]) {  // no weighted source in this tile
+        slot[s] = -1;
+        continue;
+      }
+      slot[s] = n;
+      tb.st_s[(size_t)tile * S + n] = s;
+      for (int p = 0; p < P; ++p) {
+        const int l = lo[s * P + p], h = hi[s * P + p];
+        const int la = floor_align(l);
+        const long long span = (long long)h - la;
+        if (span > 0xFFFF) wide = 1;
+        const int sp32 = (int)min(span, (long long)INT_MAX);
+        tb.st_lo[((size_t)tile * S + n) * P + p] = la;
+        tb.st_spread[((size_t)tile * S + n) * P + p] = sp32;
+        spread_max = max(spread_max, sp32);
+        mn = min(mn, l);
+        mx = max(mx, h);
+        lo_al_min = min(lo_al_min, la);
+      }
+      ++n;
+    }
+    n_active_sh = n;
+    tb.tile_hdr[tile] = make_int2(n, 0);
+    if (n > 0) {
+      atomicMin(&tb.stats[kStatMinDelay], mn);
+      atomicMax(&tb.stats[kStatMaxDelay], mx);
+      atomicMin(&tb.stats[kStatMinLoAligned], lo_al_min);
+    }
+    atomicMax(&tb.stats[kStatMaxSpread], spread_max);
+    atomicMax(&tb.stats[kStatMaxActive], n);
+    if (wide) atomicOr(&tb.stats[kStatWideTile], 1);
+  }
+  __syncthreads();
+  // 4. per (active station, source): weight and 16-bit offsets.
+  const int n_active = n_active_sh;
+  M* meta = reinterpret_cast<M*>(tb.meta) + (size_t)tile * S * K;
+  for (int idx = threadIdx.x; idx < n_active * K; idx += blockDim.x) {
+    const int j = idx / K, k = idx - j * K;
+    const int s = tb.st_s[(size_t)tile * S + j];
+    const int o = orig_of(k);
+    float w = 0.0f;
+    uint32_t off[4] = {0u, 0u, 0u, 0u};
+    if (o >= 0) {
+      w = weights[(size_t)o * S + s];
+      if (w != 0.0f) {
+        for (int p = 0; p < P; ++p) {
+          const long long v = (long long)delays[(size_t)o * S * P + s * P + p] -
+                              tb.st_lo[((size_t)tile * S + j) * P + p];
+          off[p] = (uint32_t)min(v, 0xFFFFll);
+        }
+      }
+    }
+    M m;
+    if constexpr (P <= 2) {
+      m.x = __float_as_uint(w);
+      m.y = off[0] | (off[1] << 16);
+    } else {
+      m.x = __float_as_uint(w);
+      m.y = off[0] | (off[1] << 16);
+      m.z = off[2] | (off[3] << 16);
+      m.w = 0u;
+    }
+    meta[(size_t)j * K + k] = m;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Staged shift-and-stack kernel (FP32 storage).
+//
+// Block = WS consumer warps + 1 producer warp, one source tile of
+// K = WS * KS sources, a contiguous chunk of time tiles of TT = 32 * MT
+// samples.  For every (time tile, active station) the producer's elected
+// lane copies the station's P delay windows, [t0 + lo, t0 + lo + W), from
+// HBM/L2 into a shared-memory ring of NSTAGE stages with 1-D bulk copies
+// (TMA engine, 16-byte aligned, completing on the stage's "full" mbarrier).
+// Consumer warp w owns sources w*KS .. w*KS+KS-1; lane l owns samples
+// t0 + l + 32*m, m < MT, so each warp-wide shared load reads 32 consecutive
+// words (one conflict-free wavefront) and the per-(source, station) metadata
+// is a broadcast.  Accumulation: acc = acc + w * u, rounded multiply then
+// rounded add, stations ascending, phases ascending (reference order).
+// After the last station of a time tile: strict-validity mask, packed key
+// per (source, sample), max over the thread's sources, then over the WS
+// warps through shared memory, then one red.global.max.u64 per sample; or,
+// for reduce='none', coalesced stores of the tile's beams.
+// ---------------------------------------------------------------------------
+struct WindowArgs {
+  const float* traces;
+  long long pitch;
+  int lpad;
+  int T;
+  int n_tt;            // time tiles covering T
+  int tiles_per_chunk; // time tiles per block
+  int n_tiles;
+  int S;
+  int rowcap;          // floats per ring row
+  int max_active;
+  int flexible;
+  const int4* src_info;
+  const int2* tile_hdr;
+  const int* st_s;
+  const int* st_lo;
+  const int* st_spread;
+  const void* meta;
+  unsigned long long* keys;
+  float* beam;
+  long long ldb;
+  int* status;
+};
+
+template <int P, int KS, int MT, int WS>
+struct WindowCfg {
+  static constexpr int K = WS * KS;
+  static constexpr int TT = 32 * MT;
+  static constexpr int kThreads = (WS + 1) * 32;
+};
+
+__host__ __device__ inline size_t align_up_sz(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+// Shared-memory carve-up, used identically by host (size) and device.
+template <int P, int KS, int MT, int WS, int NSTAGE, bool MAXRED>
+struct WindowSmem {
+  using M = typename MetaT<P>::type;
+  static constexpr int K = WS * KS;
+  static constexpr int TT = 32 * MT;
+  size_t ring, meta, red, srci, st_s, st_lo, st_w, bars, abort_flag, total;
+  __host__ __device__ WindowSmem(int rowcap, int max_active) {
+    size_t o = 0;
+    ring = o;        o += (size_t)NSTAGE * P * rowcap * sizeof(float);
+    o = align_up_sz(o, 16);
+    meta = o;        o += (size_t)max_active * K * sizeof(M);
+    o = align_up_sz(o, 16);
+    red = o;         o += MAXRED ? (size_t)WS * TT * sizeof(unsigned long long) : 0;
+    o = align_up_sz(o, 16);
+    srci = o;        o += (size_t)K * sizeof(int4);
+    st_s = o;        o += (size_t)max_active * sizeof(int);
+    st_lo = o;       o += (size_t)max_active * P * sizeof(int);
+    st_w = o;        o += (size_t)max_active * P * sizeof(int);
+    o = align_up_sz(o, 8);
+    bars = o;        o += (size_t)2 * NSTAGE * sizeof(uint64_t);
+    abort_flag = o;  o += 16;
+    total = align_up_sz(o, 128);
+  }
+};
+
+template <int P, int KS, int MT, int WS, int NSTAGE, bool MAXRED, bool CHECKED>
+__global__ void __launch_bounds__((WS + 1) * 32)
+beam_window_kernel(const WindowArgs a) {
+  using M = typename MetaT<P>::type;
+  constexpr int K = WS * KS;
+  constexpr int TT = 32 * MT;
+  constexpr int NCONS = WS * 32;
+  extern __shared__ __align__(128) unsigned char smem[];
+  const WindowSmem<P, KS, MT, WS, NSTAGE, MAXRED> L(a.rowcap, a.max_active);
+  float* ring = reinterpret_cast<float*>(smem + L.ring);
+  M* meta_s = reinterpret_cast<M*>(smem + L.meta);
+  unsigned long long* red = reinterpret_cast<unsigned long long*>(smem + L.red);
+  int4* srci = reinterpret_cast<int4*>(smem + L.srci);
+  int* st_s = reinterpret_cast<int*>(smem + L.st_s);
+  int* st_lo = reinterpret_cast<int*>(smem + L.st_lo);
+  int* st_w = reinterpret_cast<int*>(smem + L.st_w);
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + L.bars);
+  uint64_t* empty = full + NSTAGE;
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(smem + L.abort_flag);
+
+  const int tile = blockIdx.x % a.n_tiles;
+  const int chunk = blockIdx.x / a.n_tiles;
+  const int tau0 = chunk * a.tiles_per_chunk;
+  const int tau1 = min(tau0 + a.tiles_per_chunk, a.n_tt);
+  const int tid = threadIdx.x;
+  const int warp = tid >> 5;
+  const int lane = tid & 31;
+  const int n_active = a.tile_hdr[tile].x;
+
+  // ---- prologue: the tile's metadata into shared memory -----------------
+  {
+    const M* gm = reinterpret_cast<const M*>(a.meta) + (size_t)tile * a.S * K;
+    for (int i = tid; i < n_active * K; i += blockDim.x) meta_s[i] = gm[i];
+    for (int i = tid; i < K; i += blockDim.x) srci[i] = a.src_info[(size_t)tile * K + i];
+    for (int i = tid; i < n_active; i += blockDim.x) {
+      st_s[i] = a.st_s[(size_t)tile * a.S + i];
+#pragma unroll
+      for (int p = 0; p < P; ++p) {
+        const size_t g = ((size_t)tile * a.S + i) * P + p;
+        st_lo[i * P + p] = a.st_lo[g];
+        const int w = (int)align_up_sz((size_t)(TT + a.st_spread[g]), kAlign);
+        st_w[i * P + p] = w;
+        if (w > a.rowcap) atomicOr(a.status, kStatusBadWindow);
+      }
+    }
+    if (tid == 0) {
+      for (int s = 0; s < NSTAGE; ++s) {
+        mbar_init(&full[s], 1);
+        mbar_init(&empty[s], WS);
+      }
+      *abort_flag = 0;
+      fence_mbar_init();
+    }
+  }
+  __syncthreads();
+
+  const int n_items = (tau1 - tau0) * n_active;
+
+  // ---- producer warp ------------------------------------------------------
+  if (warp == WS) {
+    if (lane == 0) {
+      int issued = 0;
+      for (int it = 0; it < n_items; ++it) {
+        const int stage = it % NSTAGE;
+        if (it >= NSTAGE &&
+            !mbar_wait_bounded(&empty[stage], ((it / NSTAGE) - 1) & 1, abort_flag, a.status))
+          break;
+        const int tau = tau0 + it / n_active;
+        const int j = it - (it / n_active) * n_active;
+        const int t0 = tau * TT;
+        const int s = st_s[j];
+        uint32_t bytes = 0;
+#pragma unroll
+        for (int p = 0; p < P; ++p) {
+          const int w = min(st_w[j * P + p], a.rowcap);
+          bytes += (uint32_t)w * 4u;
+        }
+        mbar_arrive_expect_tx(&full[stage], bytes);
+#pragma unroll
+        for (int p = 0; p < P; ++p) {
+          const int w = min(st_w[j * P + p], a.rowcap);
+          const float* src = a.traces + (size_t)(s * P + p) * a.pitch +
+                             (long long)(a.lpad + t0 + st_lo[j * P + p]);
+          bulk_g2s(ring + (size_t)(stage * P + p) * a.rowcap, src, (uint32_t)w * 4u,
+                   &full[stage]);
+        }
+        ++issued;
+      }
+      if (*abort_flag) {
+        // Let every copy already issued land before the block can exit.
+        volatile int never = 0;
+        for (int it = max(0, issued - NSTAGE); it < issued; ++it)
+          mbar_wait_bounded(&full[it % NSTAGE], (it / NSTAGE) & 1, &never, nullptr);
+      }
+    }
+    return;
+  }
+
+  // ---- consumer warps -----------------------------------------------------
+  const int4* my_src = srci + warp * KS;
+  int it = 0;
+  for (int tau = tau0; tau < tau1; ++tau) {
+    float acc[KS][MT];
+#pragma unroll
+    for (int k = 0; k < KS; ++k)
+#pragma unroll
+      for (int m = 0; m < MT; ++m) acc[k][m] = 0.0f;
+    const int t0 = tau * TT;
+
+    for (int j = 0; j < n_active; ++j, ++it) {
+      const int stage = it % NSTAGE;
+      mbar_wait_bounded(&full[stage], (it / NSTAGE) & 1, abort_flag, a.status);
+      const float* rb = ring + (size_t)stage * P * a.rowcap + lane;
+      const M* mrow = meta_s + (size_t)j * K + warp * KS;
+#pragma unroll
+      for (int k = 0; k < KS; ++k) {
+        const M m = mrow[k];
+        const float w = __uint_as_float(m.x);
+        if (w == 0.0f) continue;  // warp-uniform: skipped station
+#pragma unroll
+        for (int p = 0; p < P; ++p) {
+          const int off = meta_off<P>(m, p);
+          const float* src = rb + p * a.rowcap + off;
+#pragma unroll
+          for (int mm = 0; mm < MT; ++mm) {
+            const float u = src[mm * 32];
+            if constexpr (CHECKED) {
+              const long long tt = (long long)t0 + lane + 32 * mm + st_lo[j * P + p] + off;
+              if (tt < 0 || tt >= a.T) continue;
+            }
+            acc[k][mm] = __fadd_rn(acc[k][mm], __fmul_rn(w, u));
+          }
+        }
+      }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&empty[stage]);
+    }
+
+    // ---- epilogue of the time tile ----
+    if constexpr (MAXRED) {
+#pragma unroll
+      for (int mm = 0; mm < MT; ++mm) {
+        const long long t = (long long)t0 + lane + 32 * mm;
+        unsigned long long best = 0ull;
+#pragma unroll
+        for (int k = 0; k < KS; ++k) {
+          const int4 si = my_src[k];
+          if (si.x < 0) continue;
+          const bool valid =
+              a.flexible ? true
+                         : (si.y <= si.z && t + si.y >= 0 && t + (long long)si.z < a.T);
+          if (!valid) continue;
+          const unsigned long long key = make_key(acc[k][mm], si.x);
+          best = key > best ? key : best;
+        }
+        red[warp * TT + lane + 32 * mm] = best;
+      }
+      named_barrier_sync(1, NCONS);
+      for (int i = tid; i < TT; i += NCONS) {
+        unsigned long long best = 0ull;
+#pragma unroll
+        for (int w = 0; w < WS; ++w) {
+          const unsigned long long v = red[w * TT + i];
+          best = v > best ? v : best;
+        }
+        if (best != 0ull && t0 + i < a.T) red_max_u64(&a.keys[t0 + i], best);
+      }
+      named_barrier_sync(1, NCONS);
+    } else {
+#pragma unroll
+      for (int k = 0; k < KS; ++k) {
+        const int4 si = my_src[k];
+        if (si.x < 0) continue;
+        float* row = a.beam + (size_t)si.x * a.ldb;
+#pragma unroll
+        for (int mm = 0; mm < MT; ++mm) {
+          const long long t = (long long)t0 + lane + 32 * mm;
+          if (t >= a.T) continue;
+          const bool valid =
+              a.flexible ? true
+                         : (si.y <= si.z && t + si.y >= 0 && t + (long long)si.z < a.T);
+          if (valid) row[t] = acc[k][mm];
+        }
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Storage element loads (direct kernel).
+// ---------------------------------------------------------------------------
+template <int STORAGE>
+__device__ __forceinline__ float load_trace(const void* base, size_t idx) {
+  if constexpr (STORAGE == BP_STORAGE_F32) {
+    return __ldg(reinterpret_cast<const float*>(base) + idx);
+  } else if constexpr (STORAGE == BP_STORAGE_BF16) {
+    return __bfloat162float(reinterpret_cast<const __nv_bfloat16*>(base)[idx]);
+  } else {
+    return __half2float(reinterpret_cast<const __half*>(base)[idx]);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Direct kernel: no staging, any P, any delay spread.  Block = 256 samples x
+// a group of sources; thread = one sample, sources looped in order.  Reads
+// the traces through L1 (coalesced along t).  Terms whose sample falls
+// outside [0, T) are skipped, which is the flexible rule and, for samples
+// the strict rule keeps, never happens.
+// ---------------------------------------------------------------------------
+struct DirectArgs {
+  const void* traces;
+  const float* scales;
+  long long pitch;
+  int lpad;
+  int T, N, S, P;
+  int flexible;
+  int src_per_block;
+  const int32_t* delays;
+  const float* weights;
+  const int32_t* minmax;   // (N, 2)
+  unsigned long long* keys;
+  float* beam;
+  long long ldb;
+};
+
+template <int STORAGE, bool MAXRED>
+__global__ void __launch_bounds__(256) beam_direct_kernel(const DirectArgs a) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int i0 = blockIdx.y * a.src_per_block;
+  const int i1 = min(i0 + a.src_per_block, a.N);
+  unsigned long long best = 0ull;
+  for (int i = i0; i < i1; ++i) {
+    const int mn = a.minmax[2 * i], mx = a.minmax[2 * i + 1];
+    const bool valid =
+        t < a.T && (a.flexible || (mn <= mx && t + mn >= 0 && t + (long long)mx < a.T));
+    float acc = 0.0f;
+    if (valid) {
+      const int32_t* d = a.delays + (size_t)i * a.S * a.P;
+      const float* wrow = a.weights + (size_t)i * a.S;
+      for (int s = 0; s < a.S; ++s) {
+        float w = __ldg(wrow + s);
+        if (w == 0.0f) continue;
+        if constexpr (STORAGE != BP_STORAGE_F32) w = w * a.scales[s];
+        for (int p = 0; p < a.P; ++p) {
+          const long long tt = t + __ldg(d + s * a.P + p);
+          if (tt < 0 || tt >= a.T) continue;
+          const float u =
+              load_trace<STORAGE>(a.traces, (size_t)(s * a.P + p) * a.pitch + a.lpad + tt);
+          acc = __fadd_rn(acc, __fmul_rn(w, u));
+        }
+      }
+    }
+    if constexpr (MAXRED) {
+      if (valid) {
+        const unsigned long long key = make_key(acc, i);
+        best = key > best ? key : best;
+      }
+    } else {
+      if (valid) a.beam[(size_t)i * a.ldb + t] = acc;
+    }
+  }
+  if constexpr (MAXRED) {
+    if (best != 0ull) red_max_u64(&a.keys[t], best);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Small kernels.
+// ---------------------------------------------------------------------------
+
+// Per-source min/max over weighted stations (beamform.c:10-47).
+__global__ void minmax_kernel(const int32_t* __restrict__ delays, const float* __restrict__ weights,
+                              int N, int S, int P, int32_t* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  int mn = INT_MAX, mx = INT_MIN;
+  const int32_t* d = delays + (size_t)i * S * P;
+  const float* w = weights + (size_t)i * S;
+  for (int s = 0; s < S; ++s) {
+    if (w[s] == 0.0f) continue;
+    for (int p = 0; p < P; ++p) {
+      const int v = d[s * P + p];
+      mn = min(mn, v);
+      mx = max(mx, v);
+    }
+  }
+  out[2 * i] = mn;
+  out[2 * i + 1] = mx;
+}
+
+// FP32 prestack into the trace layout (beamform.c:108-152 arithmetic):
+// U = ((0 + a0 * F0) + a1 * F1) + ..., rounded multiply then rounded add.
+// grid (ceil(pitch / 256), S); each thread one row index of every phase row.
+__global__ void prestack_f32_kernel(const float* __restrict__ F, const float* __restrict__ alpha,
+                                    int T, int S, int C, int P, int lpad, long long pitch,
+                                    float* __restrict__ out) {
+  const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int s = blockIdx.y;
+  if (r >= pitch) return;
+  const long long t = r - lpad;
+  const bool in = t >= 0 && t < T;
+  for (int p = 0; p < P; ++p) {
+    float acc = 0.0f;
+    if (in) {
+      for (int c = 0; c < C; ++c)
+        acc = __fadd_rn(acc, __fmul_rn(__ldg(alpha + ((size_t)s * C + c) * P + p),
+                                       __ldg(F + ((size_t)s * C + c) * T + t)));
+    }
+    out[(size_t)(s * P + p) * pitch + r] = acc;
+  }
+}
+
+// Prestacked (S, T, P) -> trace layout, FP32.
+__global__ void traces_from_prestacked_kernel(const float* __restrict__ U, int T, int S, int P,
+                                              int lpad, long long pitch, float* __restrict__ out) {
+  const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int s = blockIdx.y;
+  if (r >= pitch) return;
+  const long long t = r - lpad;
+  const bool in = t >= 0 && t < T;
+  for (int p = 0; p < P; ++p)
+    out[(size_t)(s * P + p) * pitch + r] = in ? U[((size_t)s * T + t) * P + p] : 0.0f;
+}
+
+// Keys -> (beam_max, argmax).  beam_max keeps its content where no source
+// was a candidate, argmax gets 0 there (beamform.c:332-334).
+__global__ void decode_keys_kernel(const unsigned long long* __restrict__ keys, int T,
+                                   float* __restrict__ beam_max, int32_t* __restrict__ argmax) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= T) return;
+  const unsigned long long k = keys[t];
+  if (k != 0ull) {
+    beam_max[t] = key_value(k);
+    argmax[t] = key_source(k);
+  } else {
+    argmax[t] = 0;
+  }
+}
+
+// Trace rows (S, P, T) -> prestacked (S, T, P), the reference's layout.
+__global__ void rows_to_prestacked_kernel(const float* __restrict__ rows, int T, int S, int P,
+                                          float* __restrict__ U) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int s = blockIdx.y;
+  if (t >= T) return;
+  for (int p = 0; p < P; ++p)
+    U[((size_t)s * T + t) * P + p] = rows[(size_t)(s * P + p) * T + t];
+}
+
+// Differential mode (beamform.c:338-394): one beam per source at the zero lag
+// t0 = (T - 1) / 2 of inter-station correlations, strict rule, written only
+// where the rule holds.  One thread per source, stations then phases in order.
+__global__ void differential_kernel(const float* __restrict__ traces, long long pitch, int lpad,
+                                    int T, const int32_t* __restrict__ delays,
+                                    const float* __restrict__ weights, int N, int S, int P,
+                                    float* __restrict__ beam) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const long long t0 = ((long long)T - 1) / 2;
+  const int32_t* d = delays + (size_t)i * S * P;
+  const float* w = weights + (size_t)i * S;
+  int mn = INT_MAX, mx = INT_MIN;
+  for (int s = 0; s < S; ++s) {
+    if (w[s] == 0.0f) continue;
+    for (int p = 0; p < P; ++p) {
+      mn = min(mn, d[s * P + p]);
+      mx = max(mx, d[s * P + p]);
+    }
+  }
+  if (mn > mx || t0 + mn < 0 || t0 + (long long)mx >= T) return;
+  float acc = 0.0f;
+  for (int s = 0; s < S; ++s) {
+    const float ws = w[s];
+    if (ws == 0.0f) continue;
+    for (int p = 0; p < P; ++p) {
+      const float u = traces[(size_t)(s * P + p) * pitch + lpad + t0 + d[s * P + p]];
+      acc = __fadd_rn(acc, __fmul_rn(ws, u));
+    }
+  }
+  beam[i] = acc;
+}
+
+}  // namespace bp

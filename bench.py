@@ -1,0 +1,489 @@
+"""Benchmark of the beamforming hot path (one JSON line on rank 0).
+
+Workload: the plain method at scale -- 400,000 sources, 60 stations,
+2 phases, 180,000 samples (1 h at 50 Hz), seeded synthetic data
+(beampower_b200.synthetic.LARGE), reduce='max', out_of_bounds='strict',
+FP32 storage.  Metric: nominal beam terms per second,
+sources x samples x stations x phases.
+
+One step = one full call of the hot path on inputs already in HBM: GPU
+prestack of the (S, 3, T) features, table build from the (N, S, P) delays and
+(N, S) weights, the staged shift-and-stack kernel with fused max/argmax, and
+the key decode.  Inputs (418 MB) are larger than L2, so no flush is needed.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+``--impl reference`` times the reference's own C/OpenMP library (compiled
+from its sources into oracle/_ref/) on the host cores, on a bounded
+source sample of the same workload.  Multi-GPU runs are replicas: every rank
+processes the whole workload (the north star has no multi-GPU split).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from beampower_b200.synthetic import LARGE, make_workload, nominal_terms  # noqa: E402
+
+MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+PROFILE_TRAFFIC = os.path.join(ROOT, "profiles", "beam_window_kernel_large.json")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--out-of-bounds", default="strict", choices=["strict", "flexible"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-ref-gpu", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    return ap.parse_args()
+
+
+def effective_terms(D, W, T, flexible):
+    """Terms the reference actually computes: weighted (station, phase) pairs
+    times the samples the validity rule keeps."""
+    P = D.shape[2]
+    mask = W != 0
+    n_w = mask.sum(axis=1).astype(np.int64)
+    if flexible:
+        # every sample, but only in-range terms: count per (source, station, phase)
+        valid = np.clip(T - np.abs(D.astype(np.int64)), 0, T) * mask[:, :, None]
+        return int(valid.sum())
+    big = np.iinfo(np.int32).max
+    dmin = np.where(mask[:, :, None], D, big).min(axis=(1, 2)).astype(np.int64)
+    dmax = np.where(mask[:, :, None], D, -big).max(axis=(1, 2)).astype(np.int64)
+    nt = np.clip(T - np.maximum(dmax, 0) - np.maximum(-dmin, 0), 0, T)
+    nt[n_w == 0] = 0
+    return int((nt * n_w * P).sum())
+
+
+def algorithmic_hbm_bytes(S, C, P, T, N):
+    """HBM bytes a call must move at least: features in, traces out and in,
+    delays and weights in, keys out."""
+    return 4 * S * C * T + 2 * 4 * S * P * T + 4 * N * S * P + 4 * N * S + 8 * T
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu_index = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu_index}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ----------------------------------------------------------------------------
+# CPU legs (the reference's C library; the only place bench.py runs oracle/)
+# ----------------------------------------------------------------------------
+
+def _cpu_sample(wl, n_sub):
+    """Every k-th source of the workload, full record length."""
+    N = wl["time_delays"].shape[0]
+    stride = max(1, N // n_sub)
+    idx = np.arange(0, N, stride)[:n_sub]
+    return (np.ascontiguousarray(wl["time_delays"][idx]),
+            np.ascontiguousarray(wl["weights_sources"][idx]))
+
+
+def time_reference_cpu(wl, oob, target_s, threads):
+    """Reference prestack + beamform_max on a source sample sized for about
+    target_s seconds.  Returns (terms/s, seconds, sources in sample)."""
+    from oracle.oracle import Reference, REF_CPU_SO, Oracle
+    kind = "reference"
+    try:
+        impl = Reference()
+    except OSError:
+        impl, kind = Oracle(), "port"
+    F, A = wl["waveform_features"], wl["weights_phases"]
+    S, C, T = F.shape
+    P = A.shape[2]
+
+    def run(n_sub):
+        D, W = _cpu_sample(wl, n_sub)
+        t0 = time.perf_counter()
+        U = impl.prestack(F, A, threads)
+        impl.beamform_max(U, D, W, oob, threads)
+        return time.perf_counter() - t0, D.shape[0]
+
+    n_sub = 64
+    dt, n = run(n_sub)
+    while dt < 1.0 and n_sub < wl["time_delays"].shape[0]:
+        n_sub *= 4
+        dt, n = run(n_sub)
+    n_sub = int(min(wl["time_delays"].shape[0], max(1, n_sub * target_s / max(dt, 1e-3))))
+    if target_s > 2 * dt:
+        dt, n = run(n_sub)
+    rate = nominal_terms(n, T, S, P) / dt
+    return rate, dt, n, kind
+
+
+def ref_gpu_baseline(wl, target_s=20.0):
+    """The reference's own CUDA path (oracle/_ref/beamform_gpu.so, built for
+    sm_100a) on one GPU, reduce='max', strict, on a source sample; run in a
+    child process (the library resets OpenMP thread counts)."""
+    from oracle.oracle import REF_GPU_SO
+    if not os.path.exists(REF_GPU_SO):
+        return {"unavailable": "oracle/_ref/beamform_gpu.so not built"}
+    code = r"""
+import sys, time, json, ctypes as ct, numpy as np
+sys.path.insert(0, %r)
+from oracle.oracle import Reference, REF_GPU_SO
+from beampower_b200.synthetic import LARGE, make_workload
+wl = make_workload(LARGE)
+F, A, D, W = wl["waveform_features"], wl["weights_phases"], wl["time_delays"], wl["weights_sources"]
+U = np.ascontiguousarray(Reference().prestack(F, A, -1))
+S, T, P = U.shape
+# Masked stations (weight 0) are not skipped by the reference's CUDA kernel
+# (beamform.cu:109-115): clamp their delays to the source's weighted minimum so
+# that every read stays inside the trace array (output-neutral on the CPU path).
+mask = W != 0
+big = np.iinfo(np.int32).max
+dmin = np.where(mask[:, :, None], D, big).min(axis=(1, 2))
+dmin = np.where(dmin == big, 0, dmin).astype(np.int32)
+D = np.where(mask[:, :, None], D, dmin[:, None, None]).astype(np.int32)
+lib = ct.CDLL(REF_GPU_SO)
+f32p, i32p, sz = ct.POINTER(ct.c_float), ct.POINTER(ct.c_int), ct.c_size_t
+lib.beamform_max.argtypes = [f32p, i32p, f32p, sz, sz, sz, sz, ct.c_int, f32p, i32p]
+lib.beamform_max.restype = None
+def run(n):
+    stride = max(1, D.shape[0] // n)
+    idx = np.arange(0, D.shape[0], stride)[:n]
+    d = np.ascontiguousarray(D[idx]); w = np.ascontiguousarray(W[idx])
+    bm = np.zeros(T, np.float32); am = np.zeros(T, np.int32)
+    t0 = time.perf_counter()
+    lib.beamform_max(U.ctypes.data_as(f32p), d.ctypes.data_as(i32p), w.ctypes.data_as(f32p),
+                     T, len(idx), S, P, 0, bm.ctypes.data_as(f32p), am.ctypes.data_as(i32p))
+    return time.perf_counter() - t0, len(idx)
+run(256)
+n = 1024
+dt, m = run(n)
+n = int(min(D.shape[0], max(256, n * %f / max(dt, 1e-3))))
+dt, m = run(n)
+print(json.dumps({"value": m * T * S * P / dt, "seconds": dt, "sources": m}))
+""" % (ROOT, target_s)
+    try:
+        out = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True,
+                             timeout=600)
+        line = [ln for ln in out.stdout.splitlines() if ln.startswith("{")]
+        if out.returncode != 0 or not line:
+            return {"unavailable": f"exit {out.returncode}: {out.stderr.strip()[-200:]}"}
+        r = json.loads(line[-1])
+        return {"value": r["value"], "unit": "beam terms/s",
+                "sample": f"{r['sources']} of 400000 sources (every k-th), all 180000 samples, "
+                          f"strict, {r['seconds']:.1f} s, end-to-end incl. H2D",
+                "kind": "reference CUDA (beamform.cu, sm_100a build, 1 GPU)"}
+    except subprocess.TimeoutExpired:
+        return {"unavailable": "timed out"}
+
+
+# ----------------------------------------------------------------------------
+
+def run_reference_arm(args, rank, world):
+    """--impl reference: rank 0 times the reference CPU library."""
+    if rank != 0:
+        return
+    wl = make_workload(LARGE)
+    S, C, T = wl["waveform_features"].shape
+    N, _, P = wl["time_delays"].shape
+    threads = os.cpu_count() or 1
+    oob = 0 if args.out_of_bounds == "strict" else 1
+    # size one step for ~6 s of CPU work
+    rate, dt, n_sub, kind = time_reference_cpu(wl, oob, 6.0, threads)
+    times = []
+    for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        from oracle.oracle import Reference, Oracle
+        impl = Reference() if kind == "reference" else Oracle()
+        D, W = _cpu_sample(wl, n_sub)
+        U = impl.prestack(wl["waveform_features"], wl["weights_phases"], threads)
+        impl.beamform_max(U, D, W, oob, threads)
+        if i >= args.warmup:
+            times.append(time.perf_counter() - t0)
+    terms = nominal_terms(n_sub, T, S, P)
+    value = terms / statistics.mean(times)
+    ms_full = nominal_terms(N, T, S, P) / value * 1e3
+    line = {
+        "impl": "reference", "metric": "beam terms/s (src x t x sta x phase)",
+        "value": value, "unit": "beam terms/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_full, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": LARGE.name, "n_sources": N, "n_stations": S, "n_phases": P,
+                   "n_samples": T, "reduce": "max", "out_of_bounds": args.out_of_bounds,
+                   "storage": "fp32", "parallelism": "replicas"},
+        "cpu_baseline": {"value": value, "unit": "beam terms/s", "cores": threads, "kind": kind,
+                         "sample": f"{n_sub} of {N} sources (every k-th), all {T} samples, "
+                                   "prestack + beamform_max per step; ms_per_step "
+                                   "extrapolated to the full workload"},
+        "e2e": {"value": value, "unit": "beam terms/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import beampower_b200 as bp
+    from beampower_b200.core import check, load_library
+    from beampower_b200.tables import TravelTimeTable, _stream_ptr
+
+    dist = world > 1
+    if dist:
+        import torch.distributed as tdist
+        from datetime import timedelta
+        tdist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    lib = load_library("gpu")
+    oob = 0 if args.out_of_bounds == "strict" else 1
+
+    wl = make_workload(LARGE)
+    F, A, D, W = (wl["waveform_features"], wl["weights_phases"], wl["time_delays"],
+                  wl["weights_sources"])
+    S, C, T = F.shape
+    N, _, P = D.shape
+    terms = nominal_terms(N, T, S, P)
+    eff = effective_terms(D, W, T, oob == 1)
+
+    dF = torch.from_numpy(F).to(dev)
+    dA = torch.from_numpy(A).to(dev)
+    dD = torch.from_numpy(D).to(dev)
+    dW = torch.from_numpy(W).to(dev)
+    stream = torch.cuda.current_stream()
+
+    # peaks of this GPU at its current clock (binding roofline of the kernel)
+    smem_gbs, fp32_tf = ctypes_double(), ctypes_double()
+    check(lib.bp_measure_peaks(_stream_ptr(), smem_gbs.ref, fp32_tf.ref))
+
+    ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+
+    def step(record):
+        e0, e1, e2, e3 = ev(), ev(), ev(), ev()
+        e0.record(stream)
+        table = TravelTimeTable(dD, dW, device=dev)
+        e1.record(stream)
+        traces = table.traces_from_features(dF, dA)
+        e2.record(stream)
+        bm, am = table.beamform_max(traces, oob)
+        e3.record(stream)
+        record.append((e0, e1, e2, e3, table, traces, bm, am))
+
+    # warm-up
+    recs = []
+    for _ in range(args.warmup):
+        step(recs)
+    torch.cuda.synchronize()
+    for r in recs:
+        r[4].close()
+    recs = []
+    launches0 = lib.bp_launch_count()
+    sampler = ClockSampler(local_rank) if rank == 0 else None
+    if dist:
+        tdist.barrier()
+    torch.cuda.synchronize()
+    if sampler:
+        sampler.start()
+        time.sleep(0.5)
+    t_start, t_end = ev(), ev()
+    t_start.record(stream)
+    for _ in range(args.steps):
+        step(recs)
+    t_end.record(stream)
+    torch.cuda.synchronize()
+    clocks = sampler.stop() if sampler else None
+    launches = lib.bp_launch_count() - launches0
+    elapsed_ms = t_start.elapsed_time(t_end)
+    if dist:
+        t = torch.tensor([elapsed_ms], device=dev)
+        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+        elapsed_ms = float(t.item())
+    table_ms = statistics.mean(r[0].elapsed_time(r[1]) for r in recs)
+    prestack_ms = statistics.mean(r[1].elapsed_time(r[2]) for r in recs)
+    kernel_ms = statistics.mean(r[2].elapsed_time(r[3]) for r in recs)
+    info = recs[0][4].info
+    # parity spot check of the last step at a few samples (cheap, GPU only):
+    # the argmax sources' beams are recomputed by the direct kernel elsewhere.
+    bm_last = recs[-1][6]
+    for r in recs:
+        r[4].close()
+    ms_per_step = elapsed_ms / args.steps
+    value = world * terms / (ms_per_step * 1e-3)
+
+    # ---- end to end through the public numpy API, pinned host inputs ----
+    pin = {k: torch.from_numpy(v).pin_memory() for k, v in
+           (("F", F), ("A", A), ("D", D), ("W", W))}
+    hF, hA, hD, hW = (pin[k].numpy() for k in ("F", "A", "D", "W"))
+    bp.beamform(hF, hD, hA, hW, reduce="max", out_of_bounds=args.out_of_bounds)
+    e2e_times = []
+    for _ in range(max(2, min(args.steps, 3))):
+        if dist:
+            tdist.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        bp.beamform(hF, hD, hA, hW, reduce="max", out_of_bounds=args.out_of_bounds)
+        e2e_times.append(time.perf_counter() - t0)
+    e2e_s = statistics.mean(e2e_times)
+    if dist:
+        t = torch.tensor([e2e_s], device=dev)
+        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    h2d = F.nbytes + A.nbytes + D.nbytes + W.nbytes
+    d2h = 8 * T
+
+    line = None
+    if rank == 0:
+        # roofline of the dominant kernel: shared-memory operand delivery,
+        # 4 B of trace per effective term
+        smem_achieved = eff * 4 / (kernel_ms * 1e-3) / 1e9
+        traffic = None
+        if os.path.exists(PROFILE_TRAFFIC):
+            with open(PROFILE_TRAFFIC) as fh:
+                prof = json.load(fh)
+            traffic = prof.get("dram_bytes_per_launch_full_size")
+        hbm_peak = None
+        if os.path.exists(MEASURED_PEAKS):
+            with open(MEASURED_PEAKS) as fh:
+                hbm_peak = json.load(fh).get("hbm_gbs")
+        hbm_bytes = algorithmic_hbm_bytes(S, C, P, T, N)
+        line = {
+            "metric": "beam terms/s (src x t x sta x phase)",
+            "value": value,
+            "unit": "beam terms/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": ms_per_step,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": LARGE.name, "n_sources": N, "n_stations": S, "n_phases": P,
+                       "n_samples": T, "reduce": "max", "out_of_bounds": args.out_of_bounds,
+                       "storage": "fp32", "parallelism": f"replicas{world}",
+                       "l2": "inputs 418 MB > L2, no flush"},
+            "effective_terms_per_step": eff,
+            "nominal_terms_per_step": terms,
+            "breakdown_ms": {"table_build": table_ms, "prestack": prestack_ms,
+                             "beam_kernel_and_decode": kernel_ms},
+            "roofline": {
+                "bound": "smem",
+                "achieved": smem_achieved,
+                "peak": smem_gbs.value,
+                "unit": "GB/s",
+                "frac": smem_achieved / smem_gbs.value,
+                "traffic": traffic,
+                "note": "shared-memory operand roof (4 B of trace per effective term), peak "
+                        "measured live by bp_measure_peaks; FP32 and HBM views below",
+                "fp32_view": {"achieved_tflops": eff * 2 / (kernel_ms * 1e-3) / 1e12,
+                              "peak_tflops": fp32_tf.value},
+                "hbm_view": {"achieved_gbs": hbm_bytes / (ms_per_step * 1e-3) / 1e9,
+                             "peak_gbs": hbm_peak, "of": "measured (MEASURED_PEAKS.json)"},
+            },
+            "table": info,
+            "e2e": {"value": world * terms / e2e_s, "unit": "beam terms/s",
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "seconds_per_step": e2e_s},
+            "gpu_launches": int(launches),
+            "clocks": clocks,
+        }
+    if dist:
+        tdist.barrier()
+        tdist.destroy_process_group()
+    if rank != 0:
+        return
+    # host-side baselines (rank 0, N = 1 only)
+    if world == 1 and not args.no_cpu_baseline:
+        rate, dt, n_sub, kind = time_reference_cpu(wl, oob, args.cpu_seconds, os.cpu_count() or 1)
+        line["cpu_baseline"] = {
+            "value": rate, "unit": "beam terms/s", "cores": os.cpu_count() or 1, "kind": kind,
+            "sample": f"{n_sub} of {N} sources (every k-th), all {T} samples, prestack + "
+                      f"beamform_max, {dt:.1f} s"}
+    if world == 1 and not args.no_ref_gpu:
+        line["ref_gpu_baseline"] = ref_gpu_baseline(wl)
+    print(json.dumps(line), flush=True)
+
+
+class ctypes_double:
+    def __init__(self):
+        import ctypes
+        self._v = ctypes.c_double(0.0)
+        self.ref = ctypes.byref(self._v)
+
+    @property
+    def value(self):
+        return self._v.value
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    if args.impl == "reference":
+        run_reference_arm(args, rank, world)
+        return
+    run_ours(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,232 @@
+/*
+ * beampower_b200 -- C-ABI of the sm_100a beamforming library
+ * (beampower_b200/lib/libbeampower_b200.so).
+ *
+ * Two groups of entry points:
+ *
+ * 1. Drop-ins for the reference's GPU library.  Same symbol names, argument
+ *    order and meaning as beampower/src/beamform_gpu.h:1-2, bound by
+ *    beampower/core.py:65-87 ("gpu" entry of LIBRARIES).  They take HOST
+ *    buffers, synchronise before returning, and return an int status (0 on
+ *    success) where the reference returned void and called exit() on errors.
+ *    A caller that ignores the return value (ctypes without restype) keeps
+ *    working unchanged.
+ *
+ * 2. Stream-ordered device entry points (prefix bp_) for callers whose data
+ *    already lives in HBM (torch tensors, the batch and stream schedulers).
+ *    Pointers are device pointers, `stream` is a cudaStream_t passed as
+ *    void*, nothing synchronises, and every function returns an int status.
+ *
+ * Conventions shared by both groups:
+ *   N = n_sources, S = n_stations, C = n_channels, P = n_phases,
+ *   T = n_samples.
+ *   time_delays (N, S, P) int32, weights (N, S) float32, row-major.
+ *   out_of_bounds: 0 = 'strict', 1 = 'flexible' (beampower/beampower.py:85-88).
+ *   Results follow the reference's CPU path (beampower/src/beamform.c):
+ *   stations ascending, phases ascending, one FP32 accumulator per
+ *   (source, sample), each term a rounded multiply then a rounded add,
+ *   zero-weight stations skipped; max/argmax keeps the lowest source index
+ *   among equal beams.
+ */
+#ifndef BEAMPOWER_B200_H
+#define BEAMPOWER_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define BP_API __attribute__((visibility("default")))
+#else
+#define BP_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define BP_OK 0
+#define BP_ERR_INVALID_ARGUMENT 1   /* sizes, pointers or options rejected   */
+#define BP_ERR_CUDA 2               /* a CUDA runtime call failed            */
+#define BP_ERR_OUT_OF_MEMORY 3      /* device allocation failed              */
+#define BP_ERR_UNSUPPORTED 4        /* shape outside what the kernels handle */
+#define BP_ERR_KERNEL 5             /* a kernel reported a failure (status)  */
+
+/* ---- trace storage types ---------------------------------------------- */
+#define BP_STORAGE_F32 0
+#define BP_STORAGE_BF16 1
+#define BP_STORAGE_F16 2
+
+/* ---- reduce ------------------------------------------------------------ */
+#define BP_REDUCE_NONE 0
+#define BP_REDUCE_MAX 1
+
+/* ======================================================================= */
+/* 1. Drop-in host-buffer entry points                                     */
+/* ======================================================================= */
+
+/* Full network response, reduce='none'.
+ * Replaces `beamform` of beampower/src/beamform.cu:462-659
+ * (declared beamform_gpu.h:1, argtypes core.py:65-75).
+ * waveform_features: the PRESTACKED traces (S, T, P) float32, phase fastest,
+ * as produced by prestack_waveform_features.  beam: (N, T) float32; entries
+ * that the strict rule does not compute keep the caller's content. */
+BP_API int beamform(float *waveform_features, int *time_delays, float *weights,
+             size_t n_samples, size_t n_sources, size_t n_stations,
+             size_t n_phases, int out_of_bounds, float *beam);
+
+/* Max and argmax over sources for every sample, reduce='max'.
+ * Replaces `beamform_max` of beampower/src/beamform.cu:207-460
+ * (declared beamform_gpu.h:2, argtypes core.py:76-87).
+ * beam_max[t] is written only where some source is a candidate; otherwise it
+ * keeps the caller's content (the reference front-end passes zeros,
+ * beampower/beampower.py:175-176).  source_index_beam_max[t] is always
+ * written (0 when there is no candidate). */
+BP_API int beamform_max(float *waveform_features, int *time_delays, float *weights,
+                 size_t n_samples, size_t n_sources, size_t n_stations,
+                 size_t n_phases, int out_of_bounds, float *beam_max,
+                 int *source_index_beam_max);
+
+/* Channel -> phase prestack on the GPU, host buffers.
+ * Same prototype as the CPU library's prestack_waveform_features
+ * (beampower/src/beamform.c:108-111, argtypes core.py:50-59); num_threads is
+ * accepted and ignored.  features (S, C, T), weights_phases (S, C, P),
+ * prestacked out (S, T, P), all float32. */
+BP_API int prestack_waveform_features(float *waveform_features, float *weights_phases,
+                               size_t n_samples, size_t n_stations,
+                               size_t n_channels, size_t n_phases,
+                               int num_threads, float *prestacked_traces);
+
+/* Whole hot path from host buffers in one call: upload, GPU prestack, table
+ * build, beamforming, download.  This is what beampower_b200.beamform()
+ * calls for numpy inputs (the reference front-end prestacks on the CPU,
+ * beampower/beampower.py:103-105; here it runs on the GPU).
+ * reduce = BP_REDUCE_MAX: beam_max (T,), argmax (T,) ; beam unused.
+ * reduce = BP_REDUCE_NONE: beam (N, T) ; beam_max / argmax unused.
+ * storage = BP_STORAGE_F32 / BF16 / F16 (16-bit storage uses a per-station
+ * scale and FP32 accumulation). */
+BP_API int bp_beamform_host(const float *waveform_features, const float *weights_phases,
+                     const int32_t *time_delays, const float *weights_sources,
+                     size_t n_samples, size_t n_sources, size_t n_stations,
+                     size_t n_channels, size_t n_phases, int out_of_bounds,
+                     int reduce, int storage, float *beam_max, int32_t *argmax,
+                     float *beam);
+
+/* ======================================================================= */
+/* 2. Stream-ordered device entry points                                   */
+/* ======================================================================= */
+
+/* A travel-time table made resident in HBM: per source tile, the active
+ * stations, each station's delay window, 16-bit delay offsets and weights,
+ * and per source the min/max delay over weighted stations.  Built once per
+ * (time_delays, weights_sources) pair and reused by every call. */
+typedef struct bp_table bp_table;
+
+typedef struct bp_table_info {
+  int64_t n_sources, n_stations, n_phases;
+  int32_t tile_sources;      /* sources per tile                          */
+  int32_t n_tiles;
+  int32_t min_delay;         /* min over weighted (source, station, phase) */
+  int32_t max_delay;         /* max over weighted (source, station, phase) */
+  int32_t max_spread;        /* widest per-tile station delay window - 1   */
+  int32_t max_active;        /* most active stations in one tile           */
+  int32_t any_nonfinite;     /* some non-zero weight is NaN or +-inf       */
+  int32_t uses_window_kernel;/* 1: staged kernel, 0: direct kernel         */
+} bp_table_info;
+
+/* Build a table from device arrays (N, S, P) int32 and (N, S) float32.
+ * Allocates device memory (stream-ordered) and synchronises `stream` once to
+ * read the table statistics back. */
+BP_API int bp_table_create(const int32_t *d_time_delays, const float *d_weights_sources,
+                    size_t n_sources, size_t n_stations, size_t n_phases,
+                    void *stream, bp_table **out_table);
+BP_API int bp_table_destroy(bp_table *table);
+BP_API int bp_table_get_info(const bp_table *table, bp_table_info *info);
+
+/* Layout of device trace storage for a table and a record length: element
+ * (s, p, t) sits at row (s * P + p) of `pitch` elements, index lpad + t;
+ * indexes outside [lpad, lpad + T) must hold zeros. */
+BP_API int bp_trace_layout(const bp_table *table, size_t n_samples, size_t *lpad,
+                    size_t *pitch);
+
+/* Prestack on device: features (S, C, T) f32, weights_phases (S, C, P) f32
+ * -> traces in the layout above (element type per `storage`; zero padding is
+ * written).  For 16-bit storage `d_scales` (S,) receives each station's
+ * max |U| (1 where it is 0) and traces hold U / scale. */
+BP_API int bp_prestack_dev(const float *d_features, const float *d_weights_phases,
+                    size_t n_samples, size_t n_stations, size_t n_channels,
+                    size_t n_phases, int storage, size_t lpad, size_t pitch,
+                    void *d_traces, float *d_scales, void *stream);
+
+/* Prestacked (S, T, P) f32 on device -> traces in the layout above (f32). */
+BP_API int bp_traces_from_prestacked_dev(const float *d_prestacked, size_t n_samples,
+                                  size_t n_stations, size_t n_phases, size_t lpad,
+                                  size_t pitch, float *d_traces, void *stream);
+
+/* Shift-and-stack with fused max/argmax over sources.  d_keys (T,) uint64 is
+ * scratch the caller provides; it is cleared here.  Results go to
+ * d_beam_max (T,) and d_argmax (T,) with the drop-in's semantics (beam_max
+ * keeps its previous content where no source is a candidate). */
+BP_API int bp_beamform_max_dev(const bp_table *table, const void *d_traces, int storage,
+                        const float *d_scales, size_t n_samples, size_t lpad,
+                        size_t pitch, int out_of_bounds,
+                        unsigned long long *d_keys, float *d_beam_max,
+                        int32_t *d_argmax, void *stream);
+
+/* Full response (N, T), row stride ldb elements. */
+BP_API int bp_beamform_dev(const bp_table *table, const void *d_traces, int storage,
+                    const float *d_scales, size_t n_samples, size_t lpad,
+                    size_t pitch, int out_of_bounds, float *d_beam, size_t ldb,
+                    void *stream);
+
+/* Per-source (min, max) delay over weighted stations, (N, 2) int32, the
+ * reference's _find_minmax_time_delays (beampower/src/beamform.c:10-47,
+ * beamform.cu:28-65). */
+BP_API int bp_minmax_dev(const int32_t *d_time_delays, const float *d_weights_sources,
+                  size_t n_sources, size_t n_stations, size_t n_phases,
+                  int32_t *d_minmax, void *stream);
+
+/* Direct (unstaged) kernel, any P and any delay spread: the path taken when
+ * a table's windows do not fit shared memory, and a cross-check. */
+BP_API int bp_beamform_max_direct_dev(const void *d_traces, int storage, const float *d_scales,
+                               size_t n_samples, size_t lpad, size_t pitch,
+                               const int32_t *d_time_delays, const float *d_weights_sources,
+                               size_t n_sources, size_t n_stations, size_t n_phases,
+                               int out_of_bounds, unsigned long long *d_keys,
+                               float *d_beam_max, int32_t *d_argmax, void *stream);
+
+/* Differential mode (reduce over inter-station correlations): one beam per
+ * source at the zero lag t0 = (T - 1) / 2, strict rule, written only where
+ * the rule holds.  Replaces the CPU-only beamform_differential of
+ * beampower/src/beamform.c:338-394 (argtypes core.py:27-37); the reference's
+ * GPU branch was a stub (beampower/beampower.py:220-223).  Host buffers;
+ * num_threads is accepted and ignored. */
+BP_API int beamform_differential(float *waveform_features, int *time_delays,
+                                 float *weights, size_t n_samples, size_t n_sources,
+                                 size_t n_stations, size_t n_phases, int num_threads,
+                                 float *beam);
+
+/* Device version of beamform_differential on traces in the layout above. */
+BP_API int bp_beamform_differential_dev(const float *d_traces, size_t n_samples, size_t lpad,
+                                        size_t pitch, const int32_t *d_time_delays,
+                                        const float *d_weights_sources, size_t n_sources,
+                                        size_t n_stations, size_t n_phases, float *d_beam,
+                                        void *stream);
+
+/* ---- diagnostics -------------------------------------------------------- */
+/* Last error message of the calling thread ("" if none). */
+BP_API const char *bp_last_error(void);
+/* Measure this GPU's shared-memory load bandwidth (GB/s, whole GPU) and
+ * FP32 FMA throughput (TFLOP/s) with short microbenchmarks on `stream`
+ * (synchronises it).  These are the rooflines of the staged kernel. */
+BP_API int bp_measure_peaks(void *stream, double *smem_gbs, double *fp32_tflops);
+/* Library version string. */
+BP_API const char *bp_version(void);
+/* Kernel launches issued by this process since load (all entry points). */
+BP_API uint64_t bp_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BEAMPOWER_B200_H */

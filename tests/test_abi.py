@@ -1,0 +1,117 @@
+"""The C-ABI library loads without a GPU and exports every entry point that
+include/*.h declares; the ctypes table binds them all; front-end argument
+errors behave like the reference's (no GPU work involved)."""
+import ctypes as ct
+import glob
+import os
+import re
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+
+
+def declared_symbols():
+    names = set()
+    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        text = open(h).read()
+        for m in re.finditer(r"BP_API\s+[\w\s\*]+?\b(\w+)\s*\(", text):
+            names.add(m.group(1))
+    return sorted(names)
+
+
+def test_header_declares_drop_ins():
+    names = declared_symbols()
+    for sym in ("beamform", "beamform_max", "prestack_waveform_features",
+                "beamform_differential", "bp_beamform_max_dev", "bp_table_create"):
+        assert sym in names
+
+
+def test_library_exports_every_declared_symbol():
+    from beampower_b200.core import LIBRARIES
+    path = LIBRARIES["gpu"]["filepath_library"]
+    assert os.path.exists(path), "build the library first (python -m beampower_b200.build)"
+    lib = ct.CDLL(path)
+    missing = [n for n in declared_symbols() if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_ctypes_table_covers_header():
+    from beampower_b200.core import SIGNATURES, load_library
+    assert set(declared_symbols()) <= set(SIGNATURES)
+    lib = load_library("gpu")
+    assert lib.bp_version().startswith(b"beampower_b200")
+
+
+def test_reference_argtypes_kept():
+    """The drop-in argtypes equal beampower/core.py:65-87 (restype added)."""
+    from beampower_b200.core import LIBRARIES
+    f32p, i32p = ct.POINTER(ct.c_float), ct.POINTER(ct.c_int)
+    assert LIBRARIES["gpu"]["beamform_argtypes"] == [
+        f32p, i32p, f32p, ct.c_size_t, ct.c_size_t, ct.c_size_t, ct.c_size_t, ct.c_int, f32p]
+    assert LIBRARIES["gpu"]["beamform_max_argtypes"] == [
+        f32p, i32p, f32p, ct.c_size_t, ct.c_size_t, ct.c_size_t, ct.c_size_t, ct.c_int, f32p,
+        i32p]
+
+
+def test_argument_errors_without_gpu():
+    """Invalid sizes are rejected before any CUDA call, with a message."""
+    from beampower_b200.core import load_library
+    lib = load_library("gpu")
+    rc = lib.bp_beamform_host(None, None, None, None, 10, 10, 0, 3, 2, 0, 1, 0, None, None, None)
+    assert rc == 1 and b"n_stations" in lib.bp_last_error()
+    rc = lib.bp_beamform_host(None, None, None, None, 10, 10, 4, 3, 2, 7, 1, 0, None, None, None)
+    assert rc == 1 and b"out_of_bounds" in lib.bp_last_error()
+
+
+def test_frontend_error_behaviour(capsys):
+    import beampower_b200 as bp
+    F = np.zeros((2, 3, 10), np.float32)
+    D = np.zeros((4, 2, 2), np.int32)
+    A = np.zeros((2, 3, 2), np.float32)
+    W = np.ones((4, 2), np.float32)
+    assert bp.beamform(F, D, A, W, out_of_bounds="loose") is None
+    assert "out_of_bounds should be" in capsys.readouterr().out
+    assert bp.beamform(F, D, A, W, mode="sideways") == 1
+    assert "Mode should either be" in capsys.readouterr().out
+    assert bp.beamform(F, D, A, W, reduce="mean") == 1      # the reference's fall-through
+    with pytest.raises(NameError):
+        bp.beamform(F, D, A, W, device="cpu")
+    with pytest.raises(NameError):
+        bp.load_library("tpu")
+
+
+def test_key_order_matches_reference_max_rule():
+    """Host restatement of the packed key: order = (value, -index), NaN and
+    values <= -FLT_MAX are not candidates, decode inverts encode."""
+    import struct
+    fmax = np.finfo(np.float32).max
+
+    def ordered(v):
+        b = struct.unpack("<I", struct.pack("<f", v))[0]
+        if b == 0x80000000:
+            b = 0
+        return (~b & 0xFFFFFFFF) if b & 0x80000000 else (b | 0x80000000)
+
+    def key(v, i):
+        if not (v > -fmax):
+            return 0
+        return (ordered(v) << 32) | (0xFFFFFFFF - i)
+
+    rng = np.random.default_rng(0)
+    vals = np.concatenate([rng.standard_normal(200).astype(np.float32) * 1e3,
+                           np.float32([0.0, -0.0, np.inf, -np.inf, np.nan, fmax, -fmax,
+                                       1e-42, -1e-42])])
+    for _ in range(200):
+        idx = rng.choice(len(vals), size=6)
+        cand = [(float(np.float32(vals[i])), j) for j, i in enumerate(idx)]
+        best, besti = -fmax, 0
+        for v, j in cand:
+            if v > best:
+                best, besti = v, j
+        k = max(key(v, j) for v, j in cand)
+        if best > -fmax:
+            assert k != 0 and 0xFFFFFFFF - (k & 0xFFFFFFFF) == besti
+        else:
+            assert k == 0
