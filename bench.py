@@ -50,6 +50,10 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ref-gpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--n-sources", type=int, default=None,
+                    help="keep only the first n sources (profiling runs on a smaller case)")
+    ap.add_argument("--profile", action="store_true",
+                    help="timed steps only: no end-to-end pass, no baselines")
     return ap.parse_args()
 
 
@@ -297,6 +301,9 @@ def run_ours(args, rank, world, local_rank):
     oob = 0 if args.out_of_bounds == "strict" else 1
 
     wl = make_workload(LARGE)
+    if args.n_sources:
+        wl["time_delays"] = np.ascontiguousarray(wl["time_delays"][:args.n_sources])
+        wl["weights_sources"] = np.ascontiguousarray(wl["weights_sources"][:args.n_sources])
     F, A, D, W = (wl["waveform_features"], wl["weights_phases"], wl["time_delays"],
                   wl["weights_sources"])
     S, C, T = F.shape
@@ -367,6 +374,14 @@ def run_ours(args, rank, world, local_rank):
         r[4].close()
     ms_per_step = elapsed_ms / args.steps
     value = world * terms / (ms_per_step * 1e-3)
+
+    if args.profile:
+        if rank == 0:
+            print(json.dumps({"profile_run": True, "ms_per_step": ms_per_step,
+                              "kernel_ms": kernel_ms, "n_sources": N}), flush=True)
+        if dist:
+            tdist.destroy_process_group()
+        return
 
     # ---- end to end through the public numpy API, pinned host inputs ----
     pin = {k: torch.from_numpy(v).pin_memory() for k, v in

@@ -18,7 +18,11 @@ NAMES = golden_small_names()
 
 
 def bits(a):
-    return np.ascontiguousarray(a, dtype=np.float32).view(np.uint32)
+    """float32 bit patterns, with every NaN mapped to one pattern: the GPU
+    returns the canonical NaN where x86 propagates the input's payload, and
+    the reference semantics only say "NaN" (it never wins a max)."""
+    a = np.ascontiguousarray(a, dtype=np.float32)
+    return np.where(np.isnan(a), np.uint32(0x7FC00000), a.view(np.uint32))
 
 
 def _fp(a):
