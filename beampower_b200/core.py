@@ -71,6 +71,8 @@ SIGNATURES = {
     "bp_beamform_differential_dev": ([_vp, _sz, _sz, _sz, _vp, _vp, _sz, _sz, _sz, _vp, _vp],
                                      _int),
     "bp_measure_peaks": ([_vp, ct.POINTER(ct.c_double), ct.POINTER(ct.c_double)], _int),
+    "bp_beamform_max_noalloc": ([_vp, _sz, _sz, _sz, _vp, _vp, _sz, _sz, _sz, _int, _vp, _vp,
+                                 _vp], _int),
     "bp_last_error": ([], ct.c_char_p),
     "bp_version": ([], ct.c_char_p),
     "bp_launch_count": ([], ct.c_uint64),
@@ -89,7 +91,9 @@ LIBRARIES = {
 # Status codes of include/beampower_b200.h
 BP_OK = 0
 STATUS_NAMES = {1: "invalid argument", 2: "CUDA error", 3: "out of device memory",
-                4: "unsupported shape", 5: "kernel failure"}
+                4: "unsupported shape", 5: "kernel failure",
+                6: "beyond the fixed scratch limit of the allocation-free entry point "
+                   "(524288 samples, 524288 sources)"}
 STORAGE = {"fp32": 0, "f32": 0, "float32": 0, "bf16": 1, "bfloat16": 1, "fp16": 2,
            "f16": 2, "float16": 2}
 REDUCE_NONE, REDUCE_MAX = 0, 1

@@ -51,6 +51,8 @@ extern "C" {
 #define BP_ERR_OUT_OF_MEMORY 3      /* device allocation failed              */
 #define BP_ERR_UNSUPPORTED 4        /* shape outside what the kernels handle */
 #define BP_ERR_KERNEL 5             /* a kernel reported a failure (status)  */
+#define BP_ERR_SCRATCH_LIMIT 6      /* size beyond the fixed scratch array of
+                                       bp_beamform_max_noalloc              */
 
 /* ---- trace storage types ---------------------------------------------- */
 #define BP_STORAGE_F32 0
@@ -194,6 +196,27 @@ BP_API int bp_beamform_max_direct_dev(const void *d_traces, int storage, const f
                                size_t n_sources, size_t n_stations, size_t n_phases,
                                int out_of_bounds, unsigned long long *d_keys,
                                float *d_beam_max, int32_t *d_argmax, void *stream);
+
+/* Allocation-free max/argmax, for callers that must not allocate device
+ * memory while they run (a service that reserves its GPU memory once at
+ * start-up, or a host program whose own allocator owns the device, where a
+ * cudaMalloc inside a library call would fail or stall the stream).  It has
+ * no counterpart in the reference.
+ * Same inputs and results as bp_beamform_max_direct_dev (FP32 traces in the
+ * row layout above, raw delays and weights), but its working memory -- one
+ * uint64 key per sample and a (min, max) delay pair per source -- lives in an
+ * 8 MiB array compiled into the library, which every GPU that loads the
+ * library keeps until the process exits.  Limits: n_samples <= 524288 and
+ * n_sources <= 524288; larger calls return BP_ERR_SCRATCH_LIMIT.  It calls
+ * no allocator.  The first call on each device looks up the array's device
+ * address (make it before any stream capture starts).  All calls share the
+ * array and it keeps the previous call's contents; each call clears what it
+ * needs, and calls that overlap on the GPU race with each other. */
+BP_API int bp_beamform_max_noalloc(const float *d_traces, size_t n_samples, size_t lpad,
+                                   size_t pitch, const int32_t *d_time_delays,
+                                   const float *d_weights_sources, size_t n_sources,
+                                   size_t n_stations, size_t n_phases, int out_of_bounds,
+                                   float *d_beam_max, int32_t *d_argmax, void *stream);
 
 /* Differential mode (reduce over inter-station correlations): one beam per
  * source at the zero lag t0 = (T - 1) / 2, strict rule, written only where
