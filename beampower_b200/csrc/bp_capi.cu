@@ -10,6 +10,7 @@
 #include <string>
 #include <vector>
 
+#include <cub/device/device_radix_sort.cuh>
 #include <cuda_runtime.h>
 
 #include "beampower_b200.h"
@@ -124,14 +125,136 @@ int launch_table_build(const int32_t* d, const float* w, bp::TableDev& tb, cudaS
 
 size_t pad256(size_t v) { return (v + 255) / 256 * 256; }
 
+// Keep freed stream-ordered allocations in the device's default pool between
+// calls (the default release threshold hands them back to the driver at every
+// synchronisation, and re-mapping hundreds of MB costs tens of ms per call).
+void retain_pool(int dev) {
+  static std::atomic<uint64_t> done{0};
+  if (dev < 0 || dev >= 64) return;
+  const uint64_t bit = 1ull << dev;
+  if (done.load() & bit) return;
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+    uint64_t thr = std::numeric_limits<uint64_t>::max();
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+  }
+  done.fetch_or(bit);
+}
+
+bool tiling_map_enabled() {
+  const char* v = std::getenv("BEAMPOWER_B200_TILING_MAP");
+  return !(v && v[0] == '0');
+}
+
+// Source order for the tiles (see split_dim_kernel): d_perm[n_tiles * K],
+// original indices, -1 past the last source.  Segment boundaries depend only
+// on N and K (children split at a multiple of K); the data decide which
+// (station, phase) delay orders each segment.
+int build_tiling_map(const int32_t* d_delays, const float* d_w, size_t N, size_t S, size_t P,
+                     int K, int n_tiles, int* d_perm, cudaStream_t st) {
+  const int total = n_tiles * K;
+  bp::iota_perm_kernel<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(d_perm, (int)N, total);
+  BP_LAUNCHED("iota_perm_kernel");
+  if ((int)N <= K || !tiling_map_enabled()) return BP_OK;
+  // Host: per level, every segment in position order (begin, end, splitting?).
+  std::vector<int> seg_b, seg_e, seg_dim0, seg_of_tile;
+  std::vector<size_t> level_seg_off, level_tile_off;
+  std::vector<std::pair<int, int>> cur = {{0, (int)N}};
+  int max_segs = 1;
+  while (true) {
+    bool any_split = false;
+    for (auto& be : cur)
+      if (be.second - be.first > K) any_split = true;
+    if (!any_split) break;
+    level_seg_off.push_back(seg_b.size());
+    level_tile_off.push_back(seg_of_tile.size());
+    std::vector<std::pair<int, int>> next;
+    const int base = (int)seg_b.size();
+    for (size_t g = 0; g < cur.size(); ++g) {
+      const int b = cur[g].first, e = cur[g].second;
+      const bool split = e - b > K;
+      seg_b.push_back(b);
+      seg_e.push_back(e);
+      seg_dim0.push_back(split ? 0 : -1);
+      for (int t = b / K; t < (e + K - 1) / K; ++t) seg_of_tile.push_back((int)g);
+      if (split) {
+        const int left = ((e - b + K - 1) / K / 2) * K;
+        next.push_back({b, b + left});
+        next.push_back({b + left, e});
+      } else {
+        next.push_back({b, e});
+      }
+    }
+    max_segs = std::max(max_segs, (int)seg_b.size() - base);
+    cur.swap(next);
+  }
+  if (level_seg_off.empty()) return BP_OK;
+  level_seg_off.push_back(seg_b.size());
+  level_tile_off.push_back(seg_of_tile.size());
+  int seg_bits = 1;
+  while ((1 << seg_bits) < max_segs) ++seg_bits;
+  size_t temp_bytes = 0;
+  {
+    cudaError_t e = cub::DeviceRadixSort::SortPairs(
+        nullptr, temp_bytes, (const unsigned long long*)nullptr, (unsigned long long*)nullptr,
+        (const int*)nullptr, (int*)nullptr, (int)N, 0, 32 + seg_bits, st);
+    if (e != cudaSuccess) return cuda_fail(e, "radix sort size query");
+  }
+  const size_t ns = seg_b.size(), nt = seg_of_tile.size();
+  const size_t o_b = 0, o_e = o_b + pad256(ns * 4), o_d = o_e + pad256(ns * 4),
+               o_t = o_d + pad256(ns * 4), o_ka = o_t + pad256(nt * 4),
+               o_kb = o_ka + pad256(N * 8), o_pb = o_kb + pad256(N * 8),
+               o_tmp = o_pb + pad256(N * 4), bytes = o_tmp + pad256(temp_bytes);
+  char* scratch = nullptr;
+  BP_CUDA(cudaMallocAsync(&scratch, bytes, st));
+  int* d_b = reinterpret_cast<int*>(scratch + o_b);
+  int* d_e = reinterpret_cast<int*>(scratch + o_e);
+  int* d_dim = reinterpret_cast<int*>(scratch + o_d);
+  int* d_tile = reinterpret_cast<int*>(scratch + o_t);
+  auto* d_ka = reinterpret_cast<unsigned long long*>(scratch + o_ka);
+  auto* d_kb = reinterpret_cast<unsigned long long*>(scratch + o_kb);
+  int* d_pb = reinterpret_cast<int*>(scratch + o_pb);
+  cudaError_t e = cudaMemcpyAsync(d_b, seg_b.data(), ns * 4, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d_e, seg_e.data(), ns * 4, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(d_dim, seg_dim0.data(), ns * 4, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(d_tile, seg_of_tile.data(), nt * 4, cudaMemcpyHostToDevice, st);
+  int* p_cur = d_perm;
+  int* p_next = d_pb;
+  for (size_t L = 0; e == cudaSuccess && L + 1 < level_seg_off.size(); ++L) {
+    const int nseg = (int)(level_seg_off[L + 1] - level_seg_off[L]);
+    int* ldim = d_dim + level_seg_off[L];
+    bp::split_dim_kernel<<<nseg, 128, 0, st>>>(d_delays, d_w, (int)S, (int)P, p_cur,
+                                               d_b + level_seg_off[L], d_e + level_seg_off[L],
+                                               ldim);
+    bp::split_keys_kernel<<<(unsigned)((N + 255) / 256), 256, 0, st>>>(
+        d_delays, (int)(S * P), (int)N, K, p_cur, d_tile + level_tile_off[L], ldim, d_ka);
+    g_launches.fetch_add(2, std::memory_order_relaxed);
+    e = cudaGetLastError();
+    if (e == cudaSuccess) {
+      size_t tb = temp_bytes;
+      e = cub::DeviceRadixSort::SortPairs(scratch + o_tmp, tb, d_ka, d_kb, p_cur, p_next, (int)N,
+                                          0, 32 + seg_bits, st);
+    }
+    std::swap(p_cur, p_next);
+  }
+  if (e == cudaSuccess && p_cur != d_perm)
+    e = cudaMemcpyAsync(d_perm, p_cur, N * 4, cudaMemcpyDeviceToDevice, st);
+  int rc = BP_OK;
+  if (e != cudaSuccess) rc = cuda_fail(e, "tiling map");
+  cudaFreeAsync(scratch, st);
+  return rc;
+}
+
 // ---- staged kernel dispatch -------------------------------------------------
-template <int P, bool MAXRED, bool CHECKED>
+template <int P, bool MAXRED, bool CHECKED, int STORAGE>
 int launch_window_p(const bp::WindowArgs& a, int dev, cudaStream_t st) {
   using L = bp::WindowSmem<P, kKS, kMT, kWS, kNStage, MAXRED>;
   const L lay(a.rowcap, a.max_active);
   if (lay.total > (size_t)device_smem_optin(dev))
     return fail(BP_ERR_UNSUPPORTED, "staged kernel needs %zu B of shared memory", lay.total);
-  auto kern = bp::beam_window_kernel<P, kKS, kMT, kWS, kNStage, MAXRED, CHECKED>;
+  auto kern = bp::beam_window_kernel<P, kKS, kMT, kWS, kNStage, MAXRED, CHECKED, STORAGE>;
   BP_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)lay.total));
   const long long n_chunks = (a.n_tt + a.tiles_per_chunk - 1) / a.tiles_per_chunk;
@@ -142,15 +265,29 @@ int launch_window_p(const bp::WindowArgs& a, int dev, cudaStream_t st) {
   return BP_OK;
 }
 
-template <bool MAXRED, bool CHECKED>
-int launch_window(int P, const bp::WindowArgs& a, int dev, cudaStream_t st) {
+template <bool MAXRED, bool CHECKED, int STORAGE>
+int launch_window_s(int P, const bp::WindowArgs& a, int dev, cudaStream_t st) {
   switch (P) {
-    case 1: return launch_window_p<1, MAXRED, CHECKED>(a, dev, st);
-    case 2: return launch_window_p<2, MAXRED, CHECKED>(a, dev, st);
-    case 3: return launch_window_p<3, MAXRED, CHECKED>(a, dev, st);
-    case 4: return launch_window_p<4, MAXRED, CHECKED>(a, dev, st);
+    case 1: return launch_window_p<1, MAXRED, CHECKED, STORAGE>(a, dev, st);
+    case 2: return launch_window_p<2, MAXRED, CHECKED, STORAGE>(a, dev, st);
+    case 3: return launch_window_p<3, MAXRED, CHECKED, STORAGE>(a, dev, st);
+    case 4: return launch_window_p<4, MAXRED, CHECKED, STORAGE>(a, dev, st);
     default: return fail(BP_ERR_UNSUPPORTED, "staged kernel supports 1..4 phases");
   }
+}
+
+template <bool MAXRED>
+int launch_window(int P, bool checked, int storage, const bp::WindowArgs& a, int dev,
+                  cudaStream_t st) {
+  if (storage == BP_STORAGE_F32)
+    return checked ? launch_window_s<MAXRED, true, BP_STORAGE_F32>(P, a, dev, st)
+                   : launch_window_s<MAXRED, false, BP_STORAGE_F32>(P, a, dev, st);
+  if (checked)
+    return fail(BP_ERR_UNSUPPORTED,
+                "non-finite weights in flexible mode need FP32 trace storage");
+  if (storage == BP_STORAGE_BF16) return launch_window_s<MAXRED, false, BP_STORAGE_BF16>(P, a, dev, st);
+  if (storage == BP_STORAGE_F16) return launch_window_s<MAXRED, false, BP_STORAGE_F16>(P, a, dev, st);
+  return fail(BP_ERR_INVALID_ARGUMENT, "unknown storage %d", storage);
 }
 
 int staged_smem_bytes(int P, bool maxred, int rowcap, int max_active) {
@@ -169,7 +306,7 @@ int staged_smem_bytes(int P, bool maxred, int rowcap, int max_active) {
 }
 
 int rowcap_for(const bp_table* t) {
-  return (int)bp::align_up_sz((size_t)(kTimeTile + t->info.max_spread), bp::kAlign);
+  return (int)bp::align_up_sz((size_t)(kTimeTile + t->info.max_spread + 1), bp::kAlign);
 }
 
 int choose_tiles_per_chunk(int n_tt, int n_tiles, int dev) {
@@ -194,11 +331,12 @@ int check_layout(const bp_table* t, size_t n_samples, size_t lpad, size_t pitch)
   return BP_OK;
 }
 
-int run_staged(const bp_table* t, const void* traces, size_t T, size_t lpad, size_t pitch,
-               int out_of_bounds, unsigned long long* keys, float* beam, size_t ldb,
-               cudaStream_t st) {
+int run_staged(const bp_table* t, const void* traces, int storage, const float* scales,
+               size_t T, size_t lpad, size_t pitch, int out_of_bounds, unsigned long long* keys,
+               float* beam, size_t ldb, cudaStream_t st) {
   bp::WindowArgs a{};
-  a.traces = reinterpret_cast<const float*>(traces);
+  a.traces = traces;
+  a.scales = scales;
   a.pitch = (long long)pitch;
   a.lpad = (int)lpad;
   a.T = (int)T;
@@ -221,12 +359,8 @@ int run_staged(const bp_table* t, const void* traces, size_t T, size_t lpad, siz
   a.status = t->status;
   if (a.n_tt == 0) return BP_OK;
   const bool checked = out_of_bounds && t->info.any_nonfinite;
-  const bool maxred = keys != nullptr;
-  if (maxred)
-    return checked ? launch_window<true, true>(t->dev.P, a, t->device, st)
-                   : launch_window<true, false>(t->dev.P, a, t->device, st);
-  return checked ? launch_window<false, true>(t->dev.P, a, t->device, st)
-                 : launch_window<false, false>(t->dev.P, a, t->device, st);
+  if (keys) return launch_window<true>(t->dev.P, checked, storage, a, t->device, st);
+  return launch_window<false>(t->dev.P, checked, storage, a, t->device, st);
 }
 
 int run_direct(const void* traces, int storage, const float* scales, size_t T, size_t lpad,
@@ -289,12 +423,7 @@ cudaStream_t host_stream() {
   if (!s || dev_of_s != dev) {
     cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
     dev_of_s = dev;
-    // Keep freed stream-ordered allocations in the pool between calls.
-    cudaMemPool_t pool;
-    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
-      uint64_t thr = std::numeric_limits<uint64_t>::max();
-      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
-    }
+    retain_pool(dev);
   }
   return s;
 }
@@ -369,6 +498,7 @@ int bp_table_create(const int32_t* d_delays, const float* d_weights, size_t N, s
   bp_table* t = new bp_table();
   std::memset(t, 0, sizeof(*t));
   BP_CUDA(cudaGetDevice(&t->device));
+  retain_pool(t->device);
   t->stream = st;
   const int K = kTileSources;
   const long long n_tiles = ((long long)N + K - 1) / K;
@@ -384,7 +514,7 @@ int bp_table_create(const int32_t* d_delays, const float* d_weights, size_t N, s
   const size_t o_stats = take(bp::kStatCount * sizeof(int));
   const size_t o_status = take(sizeof(int));
   const size_t o_minmax = take(N * 2 * sizeof(int32_t));
-  size_t o_src = 0, o_hdr = 0, o_sts = 0, o_stlo = 0, o_stsp = 0, o_meta = 0;
+  size_t o_src = 0, o_hdr = 0, o_sts = 0, o_stlo = 0, o_stsp = 0, o_meta = 0, o_perm = 0;
   if (window && n_tiles > 0) {
     o_src = take((size_t)n_tiles * K * sizeof(int4));
     o_hdr = take((size_t)n_tiles * sizeof(int2));
@@ -392,6 +522,7 @@ int bp_table_create(const int32_t* d_delays, const float* d_weights, size_t N, s
     o_stlo = take((size_t)n_tiles * S * P * sizeof(int));
     o_stsp = take((size_t)n_tiles * S * P * sizeof(int));
     o_meta = take((size_t)n_tiles * S * K * meta_elem);
+    o_perm = take((size_t)n_tiles * K * sizeof(int));
   }
   cudaError_t e = cudaMallocAsync(&t->mem, off, st);
   if (e != cudaSuccess) {
@@ -414,8 +545,8 @@ int bp_table_create(const int32_t* d_delays, const float* d_weights, size_t N, s
     t->dev.st_lo = reinterpret_cast<int*>(base + o_stlo);
     t->dev.st_spread = reinterpret_cast<int*>(base + o_stsp);
     t->dev.meta = base + o_meta;
+    t->dev.perm = reinterpret_cast<int*>(base + o_perm);
   }
-  t->dev.perm = nullptr;
 
   auto bail = [&](int rc) {
     bp_table_destroy(t);
@@ -432,6 +563,9 @@ int bp_table_create(const int32_t* d_delays, const float* d_weights, size_t N, s
     return bail(cuda_fail(le, "launch minmax_kernel"));
   int rc = BP_OK;
   if (window && n_tiles > 0) {
+    rc = build_tiling_map(d_delays, d_weights, N, S, P, K, (int)n_tiles,
+                          const_cast<int*>(t->dev.perm), st);
+    if (rc) return bail(rc);
     switch (P) {
       case 1: rc = launch_table_build<1>(d_delays, d_weights, t->dev, st); break;
       case 2: rc = launch_table_build<2>(d_delays, d_weights, t->dev, st); break;
@@ -458,7 +592,7 @@ int bp_table_create(const int32_t* d_delays, const float* d_weights, size_t N, s
   in.any_nonfinite = stats[bp::kStatNonFinite];
   bool use_window = window && n_tiles > 0 && !stats[bp::kStatWideTile];
   if (use_window) {
-    const int rowcap = (int)bp::align_up_sz((size_t)(kTimeTile + in.max_spread), bp::kAlign);
+    const int rowcap = (int)bp::align_up_sz((size_t)(kTimeTile + in.max_spread + 1), bp::kAlign);
     const int need = staged_smem_bytes((int)P, true, rowcap, std::max(1, in.max_active));
     if (need > device_smem_optin(t->device)) use_window = false;
   }
@@ -542,13 +676,33 @@ int bp_prestack_dev(const float* F, const float* alpha, size_t T, size_t S, size
   if (pitch < lpad + T) return fail(BP_ERR_INVALID_ARGUMENT, "pitch < lpad + n_samples");
   if (!traces || (T > 0 && (!F || !alpha)))
     return fail(BP_ERR_INVALID_ARGUMENT, "NULL pointer");
-  if (storage != BP_STORAGE_F32)
-    return fail(BP_ERR_UNSUPPORTED, "16-bit storage not built in this version");
-  (void)scales;
+  cudaStream_t st = as_stream(stream);
   dim3 grid((unsigned)((pitch + 255) / 256), (unsigned)S);
-  bp::prestack_f32_kernel<<<grid, 256, 0, as_stream(stream)>>>(
-      F, alpha, (int)T, (int)S, (int)C, (int)P, (int)lpad, (long long)pitch,
-      reinterpret_cast<float*>(traces));
+  if (storage == BP_STORAGE_F32) {
+    bp::prestack_f32_kernel<<<grid, 256, 0, st>>>(F, alpha, (int)T, (int)S, (int)C, (int)P,
+                                                  (int)lpad, (long long)pitch,
+                                                  reinterpret_cast<float*>(traces));
+  } else {
+    if (!scales) return fail(BP_ERR_INVALID_ARGUMENT, "16-bit storage needs a scales buffer");
+    if (lpad % 2) return fail(BP_ERR_INVALID_ARGUMENT, "16-bit storage needs an even lpad");
+    unsigned int* sb = reinterpret_cast<unsigned int*>(scales);
+    BP_CUDA(cudaMemsetAsync(sb, 0, S * sizeof(float), st));
+    dim3 g1((unsigned)((T + 255) / 256), (unsigned)S);
+    if (T > 0) bp::prestack_absmax_kernel<<<g1, 256, 0, st>>>(F, alpha, (int)T, (int)S, (int)C,
+                                                             (int)P, sb);
+    bp::scale_pow2_kernel<<<(unsigned)((S + 255) / 256), 256, 0, st>>>(sb, (int)S);
+    g_launches.fetch_add(2, std::memory_order_relaxed);
+    if (storage == BP_STORAGE_BF16)
+      bp::prestack_h16_kernel<BP_STORAGE_BF16><<<grid, 256, 0, st>>>(
+          F, alpha, (int)T, (int)S, (int)C, (int)P, (int)lpad, (long long)pitch, scales,
+          reinterpret_cast<__nv_bfloat16*>(traces));
+    else if (storage == BP_STORAGE_F16)
+      bp::prestack_h16_kernel<BP_STORAGE_F16><<<grid, 256, 0, st>>>(
+          F, alpha, (int)T, (int)S, (int)C, (int)P, (int)lpad, (long long)pitch, scales,
+          reinterpret_cast<__half*>(traces));
+    else
+      return fail(BP_ERR_INVALID_ARGUMENT, "unknown storage %d", storage);
+  }
   BP_LAUNCHED("prestack_f32_kernel");
   return BP_OK;
 }
@@ -584,10 +738,9 @@ int bp_beamform_max_dev(const bp_table* t, const void* traces, int storage, cons
   cudaStream_t st = as_stream(stream);
   BP_CUDA(cudaMemsetAsync(keys, 0, T * sizeof(unsigned long long), st));
   int rc;
-  if (t->info.uses_window_kernel && storage == BP_STORAGE_F32) {
-    rc = run_staged(t, traces, T, lpad, pitch, out_of_bounds, keys, nullptr, 0, st);
-  } else if (t->info.uses_window_kernel) {
-    rc = fail(BP_ERR_UNSUPPORTED, "16-bit storage is not built in this version");
+  if (t->info.uses_window_kernel) {
+    rc = run_staged(t, traces, storage, scales, T, lpad, pitch, out_of_bounds, keys, nullptr, 0,
+                    st);
   } else {
     rc = run_direct(traces, storage, scales, T, lpad, pitch, t->delays, t->weights, t->minmax,
                     t->info.n_sources, t->info.n_stations, t->info.n_phases, out_of_bounds, keys,
@@ -614,11 +767,9 @@ int bp_beamform_dev(const bp_table* t, const void* traces, int storage, const fl
   if (storage != BP_STORAGE_F32 && !scales)
     return fail(BP_ERR_INVALID_ARGUMENT, "16-bit storage needs scales");
   if (int rc = check_layout(t, T, lpad, pitch)) return rc;
-  if (t->info.uses_window_kernel && storage == BP_STORAGE_F32)
-    return run_staged(t, traces, T, lpad, pitch, out_of_bounds, nullptr, beam, ldb,
-                      as_stream(stream));
   if (t->info.uses_window_kernel)
-    return fail(BP_ERR_UNSUPPORTED, "16-bit storage is not built in this version");
+    return run_staged(t, traces, storage, scales, T, lpad, pitch, out_of_bounds, nullptr, beam,
+                      ldb, as_stream(stream));
   return run_direct(traces, storage, scales, T, lpad, pitch, t->delays, t->weights, t->minmax,
                     t->info.n_sources, t->info.n_stations, t->info.n_phases, out_of_bounds,
                     nullptr, beam, ldb, as_stream(stream));
@@ -668,15 +819,18 @@ namespace {
 // layout (from prestacked traces or from raw features).
 template <class Fill>
 int host_path(cudaStream_t st, DevBufs& bufs, const int32_t* d_delays, const float* d_w,
-              size_t T, size_t N, size_t S, size_t P, int oob, int reduce, Fill traces_fill,
-              float* beam_max, int32_t* argmax, float* beam) {
+              size_t T, size_t N, size_t S, size_t P, int oob, int reduce, int storage,
+              Fill traces_fill, float* beam_max, int32_t* argmax, float* beam) {
   TableGuard tg;
   if (int rc = bp_table_create(d_delays, d_w, N, S, P, st, &tg.t)) return rc;
   size_t lpad = 0, pitch = 0;
   if (int rc = bp_trace_layout(tg.t, T, &lpad, &pitch)) return rc;
-  float* d_traces = nullptr;
-  BP_CUDA(bufs.alloc(&d_traces, S * P * pitch * sizeof(float)));
-  if (int rc = traces_fill(d_traces, lpad, pitch)) return rc;
+  // FP32: S*P rows of 4-byte elements; 16-bit: 2*S*P rows of 2-byte elements
+  void* d_traces = nullptr;
+  float* d_scales = nullptr;
+  BP_CUDA(bufs.alloc(&d_traces, S * P * pitch * 4));
+  BP_CUDA(bufs.alloc(&d_scales, S * sizeof(float)));
+  if (int rc = traces_fill(d_traces, d_scales, lpad, pitch)) return rc;
   if (reduce == BP_REDUCE_MAX) {
     unsigned long long* d_keys = nullptr;
     float* d_bm = nullptr;
@@ -684,7 +838,7 @@ int host_path(cudaStream_t st, DevBufs& bufs, const int32_t* d_delays, const flo
     BP_CUDA(bufs.alloc(&d_keys, T * sizeof(unsigned long long)));
     BP_CUDA(bufs.alloc(&d_bm, T * sizeof(float)));
     BP_CUDA(bufs.alloc(&d_am, T * sizeof(int32_t)));
-    if (int rc = bp_beamform_max_dev(tg.t, d_traces, BP_STORAGE_F32, nullptr, T, lpad, pitch, oob,
+    if (int rc = bp_beamform_max_dev(tg.t, d_traces, storage, d_scales, T, lpad, pitch, oob,
                                      d_keys, d_bm, d_am, st))
       return rc;
     std::vector<unsigned long long> keys(T);
@@ -697,8 +851,8 @@ int host_path(cudaStream_t st, DevBufs& bufs, const int32_t* d_delays, const flo
     BP_CUDA(bufs.alloc(&d_beam, std::max<size_t>(N * T, 1) * sizeof(float)));
     // entries the strict rule leaves alone keep the caller's content
     BP_CUDA(cudaMemcpyAsync(d_beam, beam, N * T * sizeof(float), cudaMemcpyHostToDevice, st));
-    if (int rc = bp_beamform_dev(tg.t, d_traces, BP_STORAGE_F32, nullptr, T, lpad, pitch, oob,
-                                 d_beam, T, st))
+    if (int rc = bp_beamform_dev(tg.t, d_traces, storage, d_scales, T, lpad, pitch, oob, d_beam,
+                                 T, st))
       return rc;
     BP_CUDA(cudaMemcpyAsync(beam, d_beam, N * T * sizeof(float), cudaMemcpyDeviceToHost, st));
     if (int rc = read_status(tg.t, st)) return rc;
@@ -734,10 +888,12 @@ int prestacked_entry(const float* U, const int* delays, const float* w, size_t T
   BP_CUDA(cudaMemcpyAsync(d_U, U, S * T * P * sizeof(float), cudaMemcpyHostToDevice, st));
   BP_CUDA(cudaMemcpyAsync(d_d, delays, N * S * P * sizeof(int32_t), cudaMemcpyHostToDevice, st));
   BP_CUDA(cudaMemcpyAsync(d_w, w, N * S * sizeof(float), cudaMemcpyHostToDevice, st));
-  auto fill = [&](float* d_traces, size_t lpad, size_t pitch) {
-    return bp_traces_from_prestacked_dev(d_U, T, S, P, lpad, pitch, d_traces, st);
+  auto fill = [&](void* d_traces, float*, size_t lpad, size_t pitch) {
+    return bp_traces_from_prestacked_dev(d_U, T, S, P, lpad, pitch,
+                                         static_cast<float*>(d_traces), st);
   };
-  return host_path(st, bufs, d_d, d_w, T, N, S, P, oob, reduce, fill, beam_max, argmax, beam);
+  return host_path(st, bufs, d_d, d_w, T, N, S, P, oob, reduce, BP_STORAGE_F32, fill, beam_max,
+                   argmax, beam);
 }
 
 }  // namespace
@@ -797,8 +953,8 @@ int bp_beamform_host(const float* F, const float* alpha, const int32_t* delays, 
   if (oob != 0 && oob != 1) return fail(BP_ERR_INVALID_ARGUMENT, "out_of_bounds must be 0 or 1");
   if (reduce != BP_REDUCE_MAX && reduce != BP_REDUCE_NONE)
     return fail(BP_ERR_INVALID_ARGUMENT, "reduce must be BP_REDUCE_MAX or BP_REDUCE_NONE");
-  if (storage != BP_STORAGE_F32)
-    return fail(BP_ERR_UNSUPPORTED, "16-bit storage is not built in this version");
+  if (storage != BP_STORAGE_F32 && storage != BP_STORAGE_BF16 && storage != BP_STORAGE_F16)
+    return fail(BP_ERR_INVALID_ARGUMENT, "unknown storage %d", storage);
   if (T == 0) return BP_OK;
   if (!F || !alpha || (N > 0 && (!delays || !w)))
     return fail(BP_ERR_INVALID_ARGUMENT, "NULL input pointer");
@@ -822,11 +978,11 @@ int bp_beamform_host(const float* F, const float* alpha, const int32_t* delays, 
   BP_CUDA(cudaMemcpyAsync(d_w, w, N * S * sizeof(float), cudaMemcpyHostToDevice, st));
   BP_CUDA(cudaMemcpyAsync(d_F, F, S * C * T * sizeof(float), cudaMemcpyHostToDevice, st));
   BP_CUDA(cudaMemcpyAsync(d_a, alpha, S * C * P * sizeof(float), cudaMemcpyHostToDevice, st));
-  auto fill = [&](float* d_traces, size_t lpad, size_t pitch) {
-    return bp_prestack_dev(d_F, d_a, T, S, C, P, BP_STORAGE_F32, lpad, pitch, d_traces, nullptr,
-                           st);
+  auto fill = [&](void* d_traces, float* d_scales, size_t lpad, size_t pitch) {
+    return bp_prestack_dev(d_F, d_a, T, S, C, P, storage, lpad, pitch, d_traces, d_scales, st);
   };
-  return host_path(st, bufs, d_d, d_w, T, N, S, P, oob, reduce, fill, beam_max, argmax, beam);
+  return host_path(st, bufs, d_d, d_w, T, N, S, P, oob, reduce, storage, fill, beam_max, argmax,
+                   beam);
 }
 
 }  // extern "C"

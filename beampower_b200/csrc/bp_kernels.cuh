@@ -228,15 +228,16 @@ __global__ void table_build_kernel(const int32_t* __restrict__ delays,
 // for reduce='none', coalesced stores of the tile's beams.
 // ---------------------------------------------------------------------------
 struct WindowArgs {
-  const float* traces;
-  long long pitch;
+  const void* traces;  // FP32 rows, or 16-bit rows in two versions (see Half16)
+  const float* scales; // per-station scale of 16-bit storage (unused for FP32)
+  long long pitch;     // elements per row
   int lpad;
   int T;
   int n_tt;            // time tiles covering T
   int tiles_per_chunk; // time tiles per block
   int n_tiles;
   int S;
-  int rowcap;          // floats per ring row
+  int rowcap;          // elements per ring row (per version for 16-bit)
   int max_active;
   int flexible;
   const int4* src_info;
@@ -260,16 +261,18 @@ struct WindowCfg {
 
 __host__ __device__ inline size_t align_up_sz(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
-// Shared-memory carve-up, used identically by host (size) and device.
+// Shared-memory carve-up, used identically by host (size) and device.  A
+// ring row holds `rowcap` FP32 elements, or `rowcap` 16-bit elements of
+// each of the two versions: 4 * rowcap bytes either way.
 template <int P, int KS, int MT, int WS, int NSTAGE, bool MAXRED>
 struct WindowSmem {
   using M = typename MetaT<P>::type;
   static constexpr int K = WS * KS;
   static constexpr int TT = 32 * MT;
-  size_t ring, meta, red, srci, st_s, st_lo, st_w, bars, abort_flag, total;
+  size_t ring, meta, red, srci, st_s, st_lo, st_w, st_sc, bars, abort_flag, total;
   __host__ __device__ WindowSmem(int rowcap, int max_active) {
     size_t o = 0;
-    ring = o;        o += (size_t)NSTAGE * P * rowcap * sizeof(float);
+    ring = o;        o += (size_t)NSTAGE * P * rowcap * 4;
     o = align_up_sz(o, 16);
     meta = o;        o += (size_t)max_active * K * sizeof(M);
     o = align_up_sz(o, 16);
@@ -279,6 +282,7 @@ struct WindowSmem {
     st_s = o;        o += (size_t)max_active * sizeof(int);
     st_lo = o;       o += (size_t)max_active * P * sizeof(int);
     st_w = o;        o += (size_t)max_active * P * sizeof(int);
+    st_sc = o;       o += (size_t)max_active * sizeof(float);
     o = align_up_sz(o, 8);
     bars = o;        o += (size_t)2 * NSTAGE * sizeof(uint64_t);
     abort_flag = o;  o += 16;
@@ -286,25 +290,72 @@ struct WindowSmem {
   }
 };
 
-template <int P, int KS, int MT, int WS, int NSTAGE, bool MAXRED, bool CHECKED>
-__global__ void __launch_bounds__((WS + 1) * 32)
+// 16-bit pair (low half = earlier sample) -> FP32 pair, and FP32 += pair.
+template <int STORAGE>
+__device__ __forceinline__ float2 h16x2_cvt(uint32_t w) {
+  float2 r;
+  if constexpr (STORAGE == BP_STORAGE_BF16)
+    asm("{\n\t.reg .b16 lo, hi;\n\tmov.b32 {lo, hi}, %2;\n\t"
+        "cvt.f32.bf16 %0, lo;\n\tcvt.f32.bf16 %1, hi;\n\t}"
+        : "=f"(r.x), "=f"(r.y) : "r"(w));
+  else
+    asm("{\n\t.reg .b16 lo, hi;\n\tmov.b32 {lo, hi}, %2;\n\t"
+        "cvt.f32.f16 %0, lo;\n\tcvt.f32.f16 %1, hi;\n\t}"
+        : "=f"(r.x), "=f"(r.y) : "r"(w));
+  return r;
+}
+
+template <int STORAGE>
+__device__ __forceinline__ void h16x2_add(float2& acc, uint32_t w) {
+  if constexpr (STORAGE == BP_STORAGE_BF16)
+    asm("{\n\t.reg .b16 lo, hi;\n\tmov.b32 {lo, hi}, %2;\n\t"
+        "add.rn.f32.bf16 %0, lo, %0;\n\tadd.rn.f32.bf16 %1, hi, %1;\n\t}"
+        : "+f"(acc.x), "+f"(acc.y) : "r"(w));
+  else
+    asm("{\n\t.reg .b16 lo, hi;\n\tmov.b32 {lo, hi}, %2;\n\t"
+        "add.rn.f32.f16 %0, lo, %0;\n\tadd.rn.f32.f16 %1, hi, %1;\n\t}"
+        : "+f"(acc.x), "+f"(acc.y) : "r"(w));
+}
+
+// Sample of accumulator half h of pair q for this lane, relative to t0.
+// FP32: lane owns samples lane + 32 m (pair q = m 2q, 2q+1);
+// 16-bit: lane owns pairs (2 lane + 64 q, 2 lane + 64 q + 1).
+template <int STORAGE>
+__device__ __forceinline__ int pair_sample(int lane, int q, int h) {
+  if constexpr (STORAGE == BP_STORAGE_F32) return lane + 64 * q + 32 * h;
+  else return 2 * lane + 64 * q + h;
+}
+
+#ifndef BP_WINDOW_MIN_BLOCKS
+#define BP_WINDOW_MIN_BLOCKS 2
+#endif
+
+template <int P, int KS, int MT, int WS, int NSTAGE, bool MAXRED, bool CHECKED, int STORAGE>
+__global__ void __launch_bounds__((WS + 1) * 32, BP_WINDOW_MIN_BLOCKS)
 beam_window_kernel(const WindowArgs a) {
+  static_assert(MT % 2 == 0 && KS % 2 == 0, "packed pairs");
+  static_assert(!(CHECKED && STORAGE != BP_STORAGE_F32), "checked variant is FP32 only");
   using M = typename MetaT<P>::type;
+  constexpr bool F32 = STORAGE == BP_STORAGE_F32;
   constexpr int K = WS * KS;
   constexpr int TT = 32 * MT;
   constexpr int NCONS = WS * 32;
+  constexpr int ESZ = F32 ? 4 : 2;  // bytes per stored element
+  constexpr int NVER = F32 ? 1 : 2; // stored versions per row
   extern __shared__ __align__(128) unsigned char smem[];
   const WindowSmem<P, KS, MT, WS, NSTAGE, MAXRED> L(a.rowcap, a.max_active);
-  float* ring = reinterpret_cast<float*>(smem + L.ring);
+  unsigned char* ring = smem + L.ring;
   M* meta_s = reinterpret_cast<M*>(smem + L.meta);
   unsigned long long* red = reinterpret_cast<unsigned long long*>(smem + L.red);
   int4* srci = reinterpret_cast<int4*>(smem + L.srci);
   int* st_s = reinterpret_cast<int*>(smem + L.st_s);
   int* st_lo = reinterpret_cast<int*>(smem + L.st_lo);
   int* st_w = reinterpret_cast<int*>(smem + L.st_w);
+  float* st_sc = reinterpret_cast<float*>(smem + L.st_sc);
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + L.bars);
   uint64_t* empty = full + NSTAGE;
   volatile int* abort_flag = reinterpret_cast<volatile int*>(smem + L.abort_flag);
+  const size_t row_bytes = (size_t)a.rowcap * 4;  // one ring row (all versions)
 
   const int tile = blockIdx.x % a.n_tiles;
   const int chunk = blockIdx.x / a.n_tiles;
@@ -321,12 +372,14 @@ beam_window_kernel(const WindowArgs a) {
     for (int i = tid; i < n_active * K; i += blockDim.x) meta_s[i] = gm[i];
     for (int i = tid; i < K; i += blockDim.x) srci[i] = a.src_info[(size_t)tile * K + i];
     for (int i = tid; i < n_active; i += blockDim.x) {
-      st_s[i] = a.st_s[(size_t)tile * a.S + i];
+      const int s = a.st_s[(size_t)tile * a.S + i];
+      st_s[i] = s;
+      st_sc[i] = F32 ? 1.0f : a.scales[s];
 #pragma unroll
       for (int p = 0; p < P; ++p) {
         const size_t g = ((size_t)tile * a.S + i) * P + p;
         st_lo[i * P + p] = a.st_lo[g];
-        const int w = (int)align_up_sz((size_t)(TT + a.st_spread[g]), kAlign);
+        const int w = (int)align_up_sz((size_t)(TT + a.st_spread[g] + 1), kAlign);
         st_w[i * P + p] = w;
         if (w > a.rowcap) atomicOr(a.status, kStatusBadWindow);
       }
@@ -347,6 +400,7 @@ beam_window_kernel(const WindowArgs a) {
   // ---- producer warp ------------------------------------------------------
   if (warp == WS) {
     if (lane == 0) {
+      const unsigned char* tr = reinterpret_cast<const unsigned char*>(a.traces);
       int issued = 0;
       for (int it = 0; it < n_items; ++it) {
         const int stage = it % NSTAGE;
@@ -359,18 +413,18 @@ beam_window_kernel(const WindowArgs a) {
         const int s = st_s[j];
         uint32_t bytes = 0;
 #pragma unroll
-        for (int p = 0; p < P; ++p) {
-          const int w = min(st_w[j * P + p], a.rowcap);
-          bytes += (uint32_t)w * 4u;
-        }
+        for (int p = 0; p < P; ++p) bytes += (uint32_t)min(st_w[j * P + p], a.rowcap) * ESZ * NVER;
         mbar_arrive_expect_tx(&full[stage], bytes);
 #pragma unroll
         for (int p = 0; p < P; ++p) {
           const int w = min(st_w[j * P + p], a.rowcap);
-          const float* src = a.traces + (size_t)(s * P + p) * a.pitch +
-                             (long long)(a.lpad + t0 + st_lo[j * P + p]);
-          bulk_g2s(ring + (size_t)(stage * P + p) * a.rowcap, src, (uint32_t)w * 4u,
-                   &full[stage]);
+          const long long col = (long long)a.lpad + t0 + st_lo[j * P + p];
+#pragma unroll
+          for (int v = 0; v < NVER; ++v) {
+            const size_t row = (size_t)(s * P + p) * NVER + v;
+            bulk_g2s(ring + (size_t)(stage * P + p) * row_bytes + (size_t)v * a.rowcap * ESZ,
+                     tr + (row * a.pitch + col) * ESZ, (uint32_t)w * ESZ, &full[stage]);
+          }
         }
         ++issued;
       }
@@ -388,35 +442,109 @@ beam_window_kernel(const WindowArgs a) {
   const int4* my_src = srci + warp * KS;
   int it = 0;
   for (int tau = tau0; tau < tau1; ++tau) {
-    float acc[KS][MT];
+    float2 acc[KS][MT / 2];  // pair q, half h: sample pair_sample(lane, q, h)
 #pragma unroll
     for (int k = 0; k < KS; ++k)
 #pragma unroll
-      for (int m = 0; m < MT; ++m) acc[k][m] = 0.0f;
+      for (int m = 0; m < MT / 2; ++m) acc[k][m] = make_float2(0.0f, 0.0f);
     const int t0 = tau * TT;
 
     for (int j = 0; j < n_active; ++j, ++it) {
       const int stage = it % NSTAGE;
       mbar_wait_bounded(&full[stage], (it / NSTAGE) & 1, abort_flag, a.status);
-      const float* rb = ring + (size_t)stage * P * a.rowcap + lane;
+      // stage base in 32-bit words; row p of the stage at + p * rowcap words
+      const int sbase = stage * P * a.rowcap;
       const M* mrow = meta_s + (size_t)j * K + warp * KS;
+      const float scale = st_sc[j];
 #pragma unroll
-      for (int k = 0; k < KS; ++k) {
-        const M m = mrow[k];
-        const float w = __uint_as_float(m.x);
-        if (w == 0.0f) continue;  // warp-uniform: skipped station
+      for (int k2 = 0; k2 < KS; k2 += 2) {
+        M mm2[2];
+        if constexpr (P <= 2) {
+          // two sources' records in one 128-bit broadcast
+          const uint4 q4 = *reinterpret_cast<const uint4*>(mrow + k2);
+          mm2[0] = make_uint2(q4.x, q4.y);
+          mm2[1] = make_uint2(q4.z, q4.w);
+        } else {
+          mm2[0] = mrow[k2];
+          mm2[1] = mrow[k2 + 1];
+        }
 #pragma unroll
-        for (int p = 0; p < P; ++p) {
-          const int off = meta_off<P>(m, p);
-          const float* src = rb + p * a.rowcap + off;
+        for (int h = 0; h < 2; ++h) {
+          const int k = k2 + h;
+          const M m = mm2[h];
+          const float w = __uint_as_float(m.x);
+          if (w == 0.0f) continue;  // warp-uniform: skipped station
+          if constexpr (!F32) {
+            // 16-bit: sum the phases in FP32, then one fused multiply-add
+            // per sample pair with c = w * scale (exact: scale is 2^k).
+            const float c = w * scale;
+            const float2 c2 = make_float2(c, c);
+            const uint32_t* src[P];
 #pragma unroll
-          for (int mm = 0; mm < MT; ++mm) {
-            const float u = src[mm * 32];
-            if constexpr (CHECKED) {
-              const long long tt = (long long)t0 + lane + 32 * mm + st_lo[j * P + p] + off;
-              if (tt < 0 || tt >= a.T) continue;
+            for (int p = 0; p < P; ++p) {
+              const int off = meta_off<P>(m, p);
+              const int v = off & 1;
+              src[p] = reinterpret_cast<const uint32_t*>(ring) + sbase + p * a.rowcap +
+                       v * (a.rowcap >> 1) + ((off - v) >> 1) + lane;
             }
-            acc[k][mm] = __fadd_rn(acc[k][mm], __fmul_rn(w, u));
+            uint32_t wd[P][MT / 2];  // all words first (see the FP32 path)
+#pragma unroll
+            for (int p = 0; p < P; ++p)
+#pragma unroll
+              for (int q = 0; q < MT / 2; ++q) wd[p][q] = src[p][32 * q];
+#pragma unroll
+            for (int q = 0; q < MT / 2; ++q) {
+              float2 ps = h16x2_cvt<STORAGE>(wd[0][q]);
+#pragma unroll
+              for (int p = 1; p < P; ++p) h16x2_add<STORAGE>(ps, wd[p][q]);
+              acc[k][q] = __ffma2_rn(c2, ps, acc[k][q]);
+            }
+          } else if constexpr (CHECKED) {
+#pragma unroll
+            for (int p = 0; p < P; ++p) {
+              const int off = meta_off<P>(m, p);
+              const float* src =
+                  reinterpret_cast<const float*>(ring) + sbase + p * a.rowcap + off + lane;
+              const long long tb = (long long)t0 + lane + st_lo[j * P + p] + off;
+#pragma unroll
+              for (int mm = 0; mm < MT; ++mm) {
+                const long long tt = tb + 32 * mm;
+                if (tt < 0 || tt >= a.T) continue;
+                const float v = __fadd_rn((mm & 1) ? acc[k][mm >> 1].y : acc[k][mm >> 1].x,
+                                          __fmul_rn(w, src[mm * 32]));
+                if (mm & 1) acc[k][mm >> 1].y = v; else acc[k][mm >> 1].x = v;
+              }
+            }
+          } else {
+            // All of this source's words first, then the arithmetic: the
+            // loads of one (source, station) are independent, and issuing
+            // them together keeps P * MT shared-memory loads in flight.
+            const float* sbf = reinterpret_cast<const float*>(ring) + sbase + lane;
+            float u[P][MT];
+#pragma unroll
+            for (int p = 0; p < P; ++p) {
+              const float* src = sbf + p * a.rowcap + meta_off<P>(m, p);
+#pragma unroll
+              for (int mm = 0; mm < MT; ++mm) u[p][mm] = src[32 * mm];
+            }
+            if (w == 1.0f) {  // warp-uniform: 1 * u == u exactly, skip the multiply
+#pragma unroll
+              for (int p = 0; p < P; ++p)
+#pragma unroll
+                for (int q = 0; q < MT / 2; ++q)
+                  acc[k][q] = add2_rn(acc[k][q], make_float2(u[p][2 * q], u[p][2 * q + 1]));
+            } else {
+              // Scalar rounded multiply then rounded add: a packed multiply
+              // followed by a packed add can be fused downstream, which would
+              // change the last bit against the reference.
+#pragma unroll
+              for (int p = 0; p < P; ++p)
+#pragma unroll
+                for (int q = 0; q < MT / 2; ++q) {
+                  acc[k][q].x = __fadd_rn(acc[k][q].x, __fmul_rn(w, u[p][2 * q]));
+                  acc[k][q].y = __fadd_rn(acc[k][q].y, __fmul_rn(w, u[p][2 * q + 1]));
+                }
+            }
           }
         }
       }
@@ -427,21 +555,25 @@ beam_window_kernel(const WindowArgs a) {
     // ---- epilogue of the time tile ----
     if constexpr (MAXRED) {
 #pragma unroll
-      for (int mm = 0; mm < MT; ++mm) {
-        const long long t = (long long)t0 + lane + 32 * mm;
-        unsigned long long best = 0ull;
+      for (int q = 0; q < MT / 2; ++q) {
 #pragma unroll
-        for (int k = 0; k < KS; ++k) {
-          const int4 si = my_src[k];
-          if (si.x < 0) continue;
-          const bool valid =
-              a.flexible ? true
-                         : (si.y <= si.z && t + si.y >= 0 && t + (long long)si.z < a.T);
-          if (!valid) continue;
-          const unsigned long long key = make_key(acc[k][mm], si.x);
-          best = key > best ? key : best;
+        for (int h = 0; h < 2; ++h) {
+          const int rel = pair_sample<STORAGE>(lane, q, h);
+          const long long t = (long long)t0 + rel;
+          unsigned long long best = 0ull;
+#pragma unroll
+          for (int k = 0; k < KS; ++k) {
+            const int4 si = my_src[k];
+            if (si.x < 0) continue;
+            const bool valid =
+                a.flexible ? true
+                           : (si.y <= si.z && t + si.y >= 0 && t + (long long)si.z < a.T);
+            if (!valid) continue;
+            const unsigned long long key = make_key(h ? acc[k][q].y : acc[k][q].x, si.x);
+            best = key > best ? key : best;
+          }
+          red[warp * TT + rel] = best;
         }
-        red[warp * TT + lane + 32 * mm] = best;
       }
       named_barrier_sync(1, NCONS);
       for (int i = tid; i < TT; i += NCONS) {
@@ -461,13 +593,16 @@ beam_window_kernel(const WindowArgs a) {
         if (si.x < 0) continue;
         float* row = a.beam + (size_t)si.x * a.ldb;
 #pragma unroll
-        for (int mm = 0; mm < MT; ++mm) {
-          const long long t = (long long)t0 + lane + 32 * mm;
-          if (t >= a.T) continue;
-          const bool valid =
-              a.flexible ? true
-                         : (si.y <= si.z && t + si.y >= 0 && t + (long long)si.z < a.T);
-          if (valid) row[t] = acc[k][mm];
+        for (int q = 0; q < MT / 2; ++q) {
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const long long t = (long long)t0 + pair_sample<STORAGE>(lane, q, h);
+            if (t >= a.T) continue;
+            const bool valid =
+                a.flexible ? true
+                           : (si.y <= si.z && t + si.y >= 0 && t + (long long)si.z < a.T);
+            if (valid) row[t] = h ? acc[k][q].y : acc[k][q].x;
+          }
         }
       }
     }
@@ -532,8 +667,9 @@ __global__ void __launch_bounds__(256) beam_direct_kernel(const DirectArgs a) {
         for (int p = 0; p < a.P; ++p) {
           const long long tt = t + __ldg(d + s * a.P + p);
           if (tt < 0 || tt >= a.T) continue;
-          const float u =
-              load_trace<STORAGE>(a.traces, (size_t)(s * a.P + p) * a.pitch + a.lpad + tt);
+          const size_t row = (STORAGE == BP_STORAGE_F32) ? (size_t)(s * a.P + p)
+                                                         : (size_t)(s * a.P + p) * 2;
+          const float u = load_trace<STORAGE>(a.traces, row * a.pitch + a.lpad + tt);
           acc = __fadd_rn(acc, __fmul_rn(w, u));
         }
       }
@@ -666,6 +802,179 @@ __global__ void differential_kernel(const float* __restrict__ traces, long long 
     }
   }
   beam[i] = acc;
+}
+
+// ---------------------------------------------------------------------------
+// Source tiling map: recursive median splits of the sources on their delay
+// vectors (a k-d tree over the (station, phase) delays), so that the 64
+// sources of a tile are close in delay space and every station's delay
+// window inside a tile is short.  Each level: pick per splitting segment the
+// (station, phase) whose weighted delays vary most (variance over up to 256
+// evenly spaced members), then one global stable radix sort of all sources
+// on (segment, delay) keys orders every splitting segment by that delay and
+// leaves finished segments in place; children split at a multiple of the
+// tile size.  Only the grouping changes: keys and outputs use the original
+// source index.
+// ---------------------------------------------------------------------------
+__global__ void split_dim_kernel(const int32_t* __restrict__ delays,
+                                 const float* __restrict__ weights, int S, int P,
+                                 const int* __restrict__ perm, const int* __restrict__ seg_begin,
+                                 const int* __restrict__ seg_end, int* __restrict__ seg_dim) {
+  const int g = blockIdx.x;
+  const int b = seg_begin[g], e = seg_end[g];
+  const int len = e - b;
+  const int D = S * P;
+  if (len <= 0 || seg_dim[g] < 0) return;  // finished segment (dim preset to -1)
+  const int n_sample = min(len, 256);
+  __shared__ double best_v[32];
+  __shared__ int best_d[32];
+  double bv = -1.0;
+  int bd = 0;
+  for (int d = threadIdx.x; d < D; d += blockDim.x) {
+    const int s = d / P;
+    double sum = 0.0, sq = 0.0;
+    int n = 0;
+    for (int j = 0; j < n_sample; ++j) {
+      const int o = perm[b + (int)(((long long)len * j) / n_sample)];
+      if (weights[(size_t)o * S + s] == 0.0f) continue;
+      const double v = (double)delays[(size_t)o * D + d];
+      sum += v;
+      sq += v * v;
+      ++n;
+    }
+    const double var = n > 1 ? (sq - sum * sum / n) / n : 0.0;
+    if (var > bv) {  // ascending d per thread: the lower d wins ties
+      bv = var;
+      bd = d;
+    }
+  }
+  for (int off = 16; off > 0; off >>= 1) {
+    const double ov = __shfl_down_sync(0xFFFFFFFFu, bv, off);
+    const int od = __shfl_down_sync(0xFFFFFFFFu, bd, off);
+    if (ov > bv || (ov == bv && od < bd)) {
+      bv = ov;
+      bd = od;
+    }
+  }
+  if ((threadIdx.x & 31) == 0) {
+    best_v[threadIdx.x >> 5] = bv;
+    best_d[threadIdx.x >> 5] = bd;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double v = -1.0;
+    int d = 0;
+    for (int w = 0; w < (int)((blockDim.x + 31) / 32); ++w)
+      if (best_v[w] > v || (best_v[w] == v && best_d[w] < d)) {
+        v = best_v[w];
+        d = best_d[w];
+      }
+    seg_dim[g] = d;
+  }
+}
+
+// Composite sort key of every source position for one level:
+// (segment index << 32) | biased delay on the segment's split dimension
+// (0 for finished segments, which therefore keep their order).
+__global__ void split_keys_kernel(const int32_t* __restrict__ delays, int D, int N, int K,
+                                  const int* __restrict__ perm,
+                                  const int* __restrict__ seg_of_tile,
+                                  const int* __restrict__ seg_dim,
+                                  unsigned long long* __restrict__ keys) {
+  const int pos = blockIdx.x * blockDim.x + threadIdx.x;
+  if (pos >= N) return;
+  const int g = seg_of_tile[pos / K];
+  const int d = seg_dim[g];
+  uint32_t low = 0u;
+  if (d >= 0) low = (uint32_t)delays[(size_t)perm[pos] * D + d] ^ 0x80000000u;
+  keys[pos] = ((unsigned long long)(uint32_t)g << 32) | low;
+}
+
+__global__ void iota_perm_kernel(int* __restrict__ perm, int N, int total) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < total) perm[i] = (i < N) ? i : -1;
+}
+
+// ---------------------------------------------------------------------------
+// 16-bit trace storage (BF16 / FP16 with a per-station scale).
+//
+// Each (station, phase) row is stored twice: version 0 holds x[t] at index
+// lpad + t, version 1 holds x[t + 1] there.  Row (s * P + p) * 2 + v of
+// `pitch` 16-bit elements.  A pair of consecutive samples (x[a], x[a + 1]) is
+// then always one aligned 32-bit word: version a & 1, index lpad + a - (a & 1).
+// The stored value is U / scale_s with scale_s a power of two >= max |U| of
+// the station (1 for an all-zero station), so the scaling itself is exact and
+// only the rounding to 16 bits loses precision.
+// ---------------------------------------------------------------------------
+template <int STORAGE> struct Half16;
+template <> struct Half16<BP_STORAGE_BF16> {
+  using T = __nv_bfloat16;
+  static __device__ __forceinline__ T from_float(float v) { return __float2bfloat16_rn(v); }
+};
+template <> struct Half16<BP_STORAGE_F16> {
+  using T = __half;
+  static __device__ __forceinline__ T from_float(float v) { return __float2half_rn(v); }
+};
+
+// Pass 1: max |U| per station (as float bits, non-negative floats order like
+// unsigned integers).  scale_bits must be zeroed first.
+__global__ void prestack_absmax_kernel(const float* __restrict__ F, const float* __restrict__ alpha,
+                                       int T, int S, int C, int P,
+                                       unsigned int* __restrict__ scale_bits) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int s = blockIdx.y;
+  float m = 0.0f;
+  if (t < T) {
+    for (int p = 0; p < P; ++p) {
+      float acc = 0.0f;
+      for (int c = 0; c < C; ++c)
+        acc = __fadd_rn(acc, __fmul_rn(__ldg(alpha + ((size_t)s * C + c) * P + p),
+                                       __ldg(F + ((size_t)s * C + c) * T + t)));
+      m = fmaxf(m, fabsf(acc));  // fmaxf drops NaN
+    }
+  }
+  for (int off = 16; off > 0; off >>= 1) m = fmaxf(m, __shfl_down_sync(0xFFFFFFFFu, m, off));
+  if ((threadIdx.x & 31) == 0 && m > 0.0f) atomicMax(scale_bits + s, __float_as_uint(m));
+}
+
+// max |U| bits -> power-of-two scale (in place, as float).
+__global__ void scale_pow2_kernel(unsigned int* __restrict__ scale_bits, int S) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= S) return;
+  const float m = __uint_as_float(scale_bits[s]);
+  float sc = 1.0f;
+  if (m > 0.0f && isfinite(m)) {
+    int e;
+    const float f = frexpf(m, &e);  // m = f * 2^e, f in [0.5, 1)
+    sc = ldexpf(1.0f, (f == 0.5f) ? e - 1 : e);
+  }
+  reinterpret_cast<float*>(scale_bits)[s] = sc;
+}
+
+// Pass 2: U / scale rounded to 16 bits, both versions, zero padding.
+template <int STORAGE>
+__global__ void prestack_h16_kernel(const float* __restrict__ F, const float* __restrict__ alpha,
+                                    int T, int S, int C, int P, int lpad, long long pitch,
+                                    const float* __restrict__ scales,
+                                    typename Half16<STORAGE>::T* __restrict__ out) {
+  using H = Half16<STORAGE>;
+  const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int s = blockIdx.y;
+  if (r >= pitch) return;
+  const float inv = 1.0f / scales[s];  // power of two: exact
+  for (int v = 0; v < 2; ++v) {
+    const long long t = r - lpad + v;
+    const bool in = t >= 0 && t < T;
+    for (int p = 0; p < P; ++p) {
+      float acc = 0.0f;
+      if (in) {
+        for (int c = 0; c < C; ++c)
+          acc = __fadd_rn(acc, __fmul_rn(__ldg(alpha + ((size_t)s * C + c) * P + p),
+                                         __ldg(F + ((size_t)s * C + c) * T + t)));
+      }
+      out[((size_t)(s * P + p) * 2 + v) * pitch + r] = H::from_float(acc * inv);
+    }
+  }
 }
 
 }  // namespace bp

@@ -103,7 +103,10 @@ class TravelTimeTable:
         st = STORAGE[storage]
         lpad, pitch = self.layout(T)
         elem = torch.float32 if st == 0 else (torch.bfloat16 if st == 1 else torch.float16)
-        buf = torch.empty((S * self.n_phases, pitch), dtype=elem, device=self.device)
+        # 16-bit storage keeps two versions of every row (the second shifted
+        # by one sample) so that any sample pair is one aligned 32-bit word
+        rows = S * self.n_phases * (1 if st == 0 else 2)
+        buf = torch.empty((rows, pitch), dtype=elem, device=self.device)
         scales = torch.ones(S, dtype=torch.float32, device=self.device)
         check(self.lib.bp_prestack_dev(F.data_ptr(), A.data_ptr(), T, S, C, self.n_phases, st,
                                        lpad, pitch, buf.data_ptr(), scales.data_ptr(),
@@ -166,7 +169,8 @@ class Traces:
 
     def to_prestacked(self, n_phases):
         """Back to the reference's (S, T, P) float32 layout (for checks)."""
-        rows = self.buf[:, self.lpad:self.lpad + self.n_samples].float()
+        buf = self.buf if self.storage == 0 else self.buf[0::2]
+        rows = buf[:, self.lpad:self.lpad + self.n_samples].float()
         if self.scales is not None and self.storage != 0:
             rows = rows * self.scales.repeat_interleave(n_phases)[:, None]
         S = rows.shape[0] // n_phases

@@ -52,6 +52,7 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--n-sources", type=int, default=None,
                     help="keep only the first n sources (profiling runs on a smaller case)")
+    ap.add_argument("--storage", default="fp32", choices=["fp32", "bf16", "fp16"])
     ap.add_argument("--profile", action="store_true",
                     help="timed steps only: no end-to-end pass, no baselines")
     return ap.parse_args()
@@ -328,7 +329,7 @@ def run_ours(args, rank, world, local_rank):
         e0.record(stream)
         table = TravelTimeTable(dD, dW, device=dev)
         e1.record(stream)
-        traces = table.traces_from_features(dF, dA)
+        traces = table.traces_from_features(dF, dA, storage=args.storage)
         e2.record(stream)
         bm, am = table.beamform_max(traces, oob)
         e3.record(stream)
@@ -378,7 +379,9 @@ def run_ours(args, rank, world, local_rank):
     if args.profile:
         if rank == 0:
             print(json.dumps({"profile_run": True, "ms_per_step": ms_per_step,
-                              "kernel_ms": kernel_ms, "n_sources": N}), flush=True)
+                              "kernel_ms": kernel_ms, "table_ms": table_ms,
+                              "prestack_ms": prestack_ms, "n_sources": N,
+                              "storage": args.storage, "table": info}), flush=True)
         if dist:
             tdist.destroy_process_group()
         return
@@ -387,14 +390,16 @@ def run_ours(args, rank, world, local_rank):
     pin = {k: torch.from_numpy(v).pin_memory() for k, v in
            (("F", F), ("A", A), ("D", D), ("W", W))}
     hF, hA, hD, hW = (pin[k].numpy() for k in ("F", "A", "D", "W"))
-    bp.beamform(hF, hD, hA, hW, reduce="max", out_of_bounds=args.out_of_bounds)
+    bp.beamform(hF, hD, hA, hW, reduce="max", out_of_bounds=args.out_of_bounds,
+                storage=args.storage)
     e2e_times = []
     for _ in range(max(2, min(args.steps, 3))):
         if dist:
             tdist.barrier()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        bp.beamform(hF, hD, hA, hW, reduce="max", out_of_bounds=args.out_of_bounds)
+        bp.beamform(hF, hD, hA, hW, reduce="max", out_of_bounds=args.out_of_bounds,
+                    storage=args.storage)
         e2e_times.append(time.perf_counter() - t0)
     e2e_s = statistics.mean(e2e_times)
     if dist:
@@ -434,7 +439,7 @@ def run_ours(args, rank, world, local_rank):
             "data": "synthetic",
             "config": {"workload": LARGE.name, "n_sources": N, "n_stations": S, "n_phases": P,
                        "n_samples": T, "reduce": "max", "out_of_bounds": args.out_of_bounds,
-                       "storage": "fp32", "parallelism": f"replicas{world}",
+                       "storage": args.storage, "parallelism": f"replicas{world}",
                        "l2": "inputs 418 MB > L2, no flush"},
             "effective_terms_per_step": eff,
             "nominal_terms_per_step": terms,

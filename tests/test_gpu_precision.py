@@ -1,0 +1,92 @@
+"""16-bit trace storage (BF16 / FP16 with a power-of-two per-station scale,
+FP32 accumulation) against the float64 restatement of the reference.
+
+Tolerances, relative to |beam| in float64 (all terms of these cases have
+one sign, so the beam's relative error is bounded by one rounding of the
+stored values):
+  FP16 storage: 1e-3 (11 significant bits: unit roundoff 2^-11 = 4.9e-4)
+  BF16 storage: 4e-3 (8 significant bits: unit roundoff 2^-8 = 3.9e-3)
+Argmax: identical wherever the float64 top-two margin exceeds the tolerance.
+"""
+import numpy as np
+import pytest
+
+from conftest import load_golden
+
+pytestmark = pytest.mark.gpu
+
+TOL = {"fp16": 1e-3, "bf16": 4e-3}
+
+
+def _margin_mask(beam64, valid, tol):
+    """Samples whose float64 winner beats the runner-up by more than tol."""
+    b = np.where(valid, beam64, -np.inf)
+    order = np.argsort(-b, axis=0)
+    top1 = np.take_along_axis(b, order[:1], axis=0)[0]
+    top2 = np.take_along_axis(b, order[1:2], axis=0)[0] if b.shape[0] > 1 else \
+        np.full_like(top1, -np.inf)
+    has = np.isfinite(top1)
+    return has & ((top1 - top2) > tol * np.abs(top1)), order[0], top1
+
+
+def _check(orc, F, A, D, W, storage, oob, sources=None):
+    import beampower_b200 as bp
+    tol = TOL[storage]
+    tag = "strict" if oob == 0 else "flexible"
+    U64 = orc.fp64_prestack(F, A)
+    beam64, valid = orc.fp64_beams(U64, D, W, oob)
+    # full response
+    beam = bp.beamform(F, D, A, W, reduce=None, out_of_bounds=tag, storage=storage)
+    big = valid & (np.abs(beam64) > 1e-6 * np.abs(beam64).max())
+    rel = np.abs(beam[big] - beam64[big]) / np.abs(beam64[big])
+    assert rel.max() <= tol, (storage, tag, rel.max())
+    assert np.all(beam[~valid] == 0)
+    # max / argmax
+    bm, am = bp.beamform(F, D, A, W, reduce="max", out_of_bounds=tag, storage=storage)
+    sure, arg64, top1 = _margin_mask(beam64, valid, tol)
+    assert np.array_equal(am[sure], arg64[sure]), (storage, tag)
+    has = np.isfinite(top1)
+    relm = np.abs(bm[has] - top1[has]) / np.maximum(np.abs(top1[has]), 1e-30)
+    assert relm.max() <= tol, (storage, tag, relm.max())
+    return rel.max(), relm.max()
+
+
+@pytest.mark.parametrize("storage", ["fp16", "bf16"])
+@pytest.mark.parametrize("name", ["random_p2", "random_p1", "random_p3", "long_delays"])
+def test_16bit_storage_within_tolerance(cuda, orc, storage, name):
+    g = load_golden(name)
+    for oob in (0, 1):
+        _check(orc, g["F"], g["A"], g["D"], g["W"], storage, oob)
+
+
+@pytest.mark.parametrize("spec_name", ["small-4k-src-20-sta-6000-samples", "small-heavy-tailed"])
+def test_16bit_storage_small_network(cuda, orc, spec_name):
+    """The 4,000-source network, Gaussian and heavy-tailed noise: the first
+    1,000 sources against float64 (both storage types, strict)."""
+    from beampower_b200.synthetic import SPECS, make_workload
+    wl = make_workload(SPECS[spec_name])
+    n = 1000
+    F, A = wl["waveform_features"], wl["weights_phases"]
+    D, W = wl["time_delays"][:n], wl["weights_sources"][:n]
+    for storage in ("fp16", "bf16"):
+        _check(orc, F, A, D, W, storage, 0)
+
+
+def test_16bit_torch_path_and_scales(cuda, orc):
+    """Device path: per-station scales are powers of two >= max |U|."""
+    import torch
+    from beampower_b200.tables import TravelTimeTable
+    g = load_golden("random_p2")
+    table = TravelTimeTable(g["D"], g["W"])
+    for storage in ("fp16", "bf16"):
+        tr = table.traces_from_features(g["F"], g["A"], storage=storage)
+        sc = tr.scales.cpu().numpy()
+        U = orc.fp64_prestack(g["F"], g["A"])
+        mx = np.abs(U).max(axis=(1, 2))
+        assert np.all(sc >= mx) and np.all(sc < 2 * mx + (mx == 0))
+        assert np.all(np.log2(sc) == np.round(np.log2(sc)))
+        back = tr.to_prestacked(g["U"].shape[2]).cpu().numpy()
+        assert np.allclose(back, U, rtol=TOL[storage], atol=1e-6 * np.abs(U).max())
+        bm, am = table.beamform_max(tr, 0)
+        torch.cuda.synchronize()
+    table.close()
