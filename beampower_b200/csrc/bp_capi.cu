@@ -58,7 +58,10 @@ constexpr long long kMaxInt = std::numeric_limits<int>::max();
 // ---- default staged-kernel configuration -----------------------------------
 // 8 consumer warps x 8 sources per thread = 64 sources per tile, 8 samples
 // per lane = 256-sample time tiles, 4-stage ring.
-constexpr int kKS = 8, kMT = 8, kWS = 8, kNStage = 4;
+#ifndef BP_NSTAGE
+#define BP_NSTAGE 4
+#endif
+constexpr int kKS = 8, kMT = 8, kWS = 8, kNStage = BP_NSTAGE;
 constexpr int kTileSources = kWS * kKS;
 constexpr int kTimeTile = 32 * kMT;
 static_assert(bp::kMaxTimeTile % kTimeTile == 0, "time tile must divide kMaxTimeTile");

@@ -369,7 +369,24 @@ beam_window_kernel(const WindowArgs a) {
   // ---- prologue: the tile's metadata into shared memory -----------------
   {
     const M* gm = reinterpret_cast<const M*>(a.meta) + (size_t)tile * a.S * K;
-    for (int i = tid; i < n_active * K; i += blockDim.x) meta_s[i] = gm[i];
+    if constexpr (F32) {
+      for (int i = tid; i < n_active * K; i += blockDim.x) meta_s[i] = gm[i];
+    } else {
+      // 16-bit: turn each sample offset into the 32-bit word offset inside
+      // the ring row, version included: (off >> 1) + (off & 1) * rowcap / 2
+      // (version 1 starts rowcap / 2 words into the row).
+      const uint32_t half_row = (uint32_t)a.rowcap >> 1;
+      for (int i = tid; i < n_active * K; i += blockDim.x) {
+        M m = gm[i];
+        auto wo = [&](uint32_t v) {
+          const uint32_t lo = v & 0xFFFFu, hi = v >> 16;
+          return ((lo >> 1) + (lo & 1u) * half_row) | (((hi >> 1) + (hi & 1u) * half_row) << 16);
+        };
+        m.y = wo(m.y);
+        if constexpr (P > 2) m.z = wo(m.z);
+        meta_s[i] = m;
+      }
+    }
     for (int i = tid; i < K; i += blockDim.x) srci[i] = a.src_info[(size_t)tile * K + i];
     for (int i = tid; i < n_active; i += blockDim.x) {
       const int s = a.st_s[(size_t)tile * a.S + i];
@@ -479,14 +496,11 @@ beam_window_kernel(const WindowArgs a) {
             // per sample pair with c = w * scale (exact: scale is 2^k).
             const float c = w * scale;
             const float2 c2 = make_float2(c, c);
-            const uint32_t* src[P];
+            const uint32_t* src[P];  // word offsets prepared in the prologue
 #pragma unroll
-            for (int p = 0; p < P; ++p) {
-              const int off = meta_off<P>(m, p);
-              const int v = off & 1;
+            for (int p = 0; p < P; ++p)
               src[p] = reinterpret_cast<const uint32_t*>(ring) + sbase + p * a.rowcap +
-                       v * (a.rowcap >> 1) + ((off - v) >> 1) + lane;
-            }
+                       meta_off<P>(m, p) + lane;
             uint32_t wd[P][MT / 2];  // all words first (see the FP32 path)
 #pragma unroll
             for (int p = 0; p < P; ++p)
@@ -494,9 +508,24 @@ beam_window_kernel(const WindowArgs a) {
               for (int q = 0; q < MT / 2; ++q) wd[p][q] = src[p][32 * q];
 #pragma unroll
             for (int q = 0; q < MT / 2; ++q) {
-              float2 ps = h16x2_cvt<STORAGE>(wd[0][q]);
+              float2 ps;
+              if constexpr (STORAGE == BP_STORAGE_F16) {
+                // phases summed in FP16 pairs (one extra FP16 rounding of a
+                // sum of values in [-P, P]), then widened once
+                __half2 hs = *reinterpret_cast<const __half2*>(&wd[0][q]);
 #pragma unroll
-              for (int p = 1; p < P; ++p) h16x2_add<STORAGE>(ps, wd[p][q]);
+                for (int p = 1; p < P; ++p)
+                  hs = __hadd2(hs, *reinterpret_cast<const __half2*>(&wd[p][q]));
+                ps = __half22float2(hs);
+              } else {
+                // BF16 -> FP32 is exact bit placement; phases summed in FP32
+                ps = make_float2(__uint_as_float(wd[0][q] << 16),
+                                 __uint_as_float(wd[0][q] & 0xFFFF0000u));
+#pragma unroll
+                for (int p = 1; p < P; ++p)
+                  ps = add2_rn(ps, make_float2(__uint_as_float(wd[p][q] << 16),
+                                               __uint_as_float(wd[p][q] & 0xFFFF0000u)));
+              }
               acc[k][q] = __ffma2_rn(c2, ps, acc[k][q]);
             }
           } else if constexpr (CHECKED) {
