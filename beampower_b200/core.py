@@ -46,6 +46,26 @@ class TableInfo(ct.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+class Record(ct.Structure):
+    """Mirror of ``bp_record`` (include/beampower_b200.h)."""
+
+    _fields_ = [
+        ("table", ct.c_int32),
+        ("out_of_bounds", ct.c_int32),
+        ("traces", ct.c_void_p),
+        ("scales", ct.c_void_p),
+        ("n_samples", ct.c_size_t),
+        ("lpad", ct.c_size_t),
+        ("pitch", ct.c_size_t),
+        ("t_origin", ct.c_int64),
+        ("out0", ct.c_size_t),
+        ("out1", ct.c_size_t),
+        ("station_mask", ct.c_void_p),
+        ("beam_max", ct.c_void_p),
+        ("argmax", ct.c_void_p),
+    ]
+
+
 # symbol -> (argtypes, restype)
 SIGNATURES = {
     # drop-ins, argtypes of beampower/core.py:65-87 (restype added: int status)
@@ -73,6 +93,11 @@ SIGNATURES = {
     "bp_measure_peaks": ([_vp, ct.POINTER(ct.c_double), ct.POINTER(ct.c_double)], _int),
     "bp_beamform_max_noalloc": ([_vp, _sz, _sz, _sz, _vp, _vp, _sz, _sz, _sz, _int, _vp, _vp,
                                  _vp], _int),
+    "bp_batch_create": ([ct.POINTER(_vp), _int, ct.POINTER(Record), _int, _int, _vp,
+                         ct.POINTER(_vp)], _int),
+    "bp_batch_run": ([_vp, _vp], _int),
+    "bp_batch_status": ([_vp, _vp, ct.POINTER(_int)], _int),
+    "bp_batch_destroy": ([_vp], _int),
     "bp_last_error": ([], ct.c_char_p),
     "bp_version": ([], ct.c_char_p),
     "bp_launch_count": ([], ct.c_uint64),

@@ -252,44 +252,59 @@ int build_tiling_map(const int32_t* d_delays, const float* d_w, size_t N, size_t
 
 // ---- staged kernel dispatch -------------------------------------------------
 template <int P, bool MAXRED, bool CHECKED, int STORAGE>
-int launch_window_p(const bp::WindowArgs& a, int dev, cudaStream_t st) {
+int launch_window_p(const bp::LaunchArgs& a, bool batch, long long plain_blocks, int dev,
+                    cudaStream_t st) {
   using L = bp::WindowSmem<P, kKS, kMT, kWS, kNStage, MAXRED>;
   const L lay(a.rowcap, a.max_active);
   if (lay.total > (size_t)device_smem_optin(dev))
     return fail(BP_ERR_UNSUPPORTED, "staged kernel needs %zu B of shared memory", lay.total);
-  auto kern = bp::beam_window_kernel<P, kKS, kMT, kWS, kNStage, MAXRED, CHECKED, STORAGE>;
-  BP_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)lay.total));
-  const long long n_chunks = (a.n_tt + a.tiles_per_chunk - 1) / a.tiles_per_chunk;
-  const long long blocks = n_chunks * a.n_tiles;
-  if (blocks > kMaxInt) return fail(BP_ERR_UNSUPPORTED, "grid too large");
-  kern<<<(unsigned)blocks, bp::WindowCfg<P, kKS, kMT, kWS>::kThreads, lay.total, st>>>(a);
-  BP_LAUNCHED("beam_window_kernel");
+  constexpr int threads = bp::WindowCfg<P, kKS, kMT, kWS>::kThreads;
+  if (batch) {
+    auto kern = bp::beam_batch_kernel<P, kKS, kMT, kWS, kNStage, MAXRED, CHECKED, STORAGE>;
+    BP_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)lay.total));
+    int per_sm = 0;
+    BP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, lay.total));
+    const int grid = std::max(1, per_sm) * std::max(1, device_sm_count(dev));
+    kern<<<grid, threads, lay.total, st>>>(a);
+    BP_LAUNCHED("beam_batch_kernel");
+  } else {
+    auto kern = bp::beam_window_kernel<P, kKS, kMT, kWS, kNStage, MAXRED, CHECKED, STORAGE>;
+    BP_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)lay.total));
+    if (plain_blocks > kMaxInt) return fail(BP_ERR_UNSUPPORTED, "grid too large");
+    if (plain_blocks <= 0) return BP_OK;
+    kern<<<(unsigned)plain_blocks, threads, lay.total, st>>>(a);
+    BP_LAUNCHED("beam_window_kernel");
+  }
   return BP_OK;
 }
 
 template <bool MAXRED, bool CHECKED, int STORAGE>
-int launch_window_s(int P, const bp::WindowArgs& a, int dev, cudaStream_t st) {
+int launch_window_s(int P, const bp::LaunchArgs& a, bool batch, long long blocks, int dev,
+                    cudaStream_t st) {
   switch (P) {
-    case 1: return launch_window_p<1, MAXRED, CHECKED, STORAGE>(a, dev, st);
-    case 2: return launch_window_p<2, MAXRED, CHECKED, STORAGE>(a, dev, st);
-    case 3: return launch_window_p<3, MAXRED, CHECKED, STORAGE>(a, dev, st);
-    case 4: return launch_window_p<4, MAXRED, CHECKED, STORAGE>(a, dev, st);
+    case 1: return launch_window_p<1, MAXRED, CHECKED, STORAGE>(a, batch, blocks, dev, st);
+    case 2: return launch_window_p<2, MAXRED, CHECKED, STORAGE>(a, batch, blocks, dev, st);
+    case 3: return launch_window_p<3, MAXRED, CHECKED, STORAGE>(a, batch, blocks, dev, st);
+    case 4: return launch_window_p<4, MAXRED, CHECKED, STORAGE>(a, batch, blocks, dev, st);
     default: return fail(BP_ERR_UNSUPPORTED, "staged kernel supports 1..4 phases");
   }
 }
 
 template <bool MAXRED>
-int launch_window(int P, bool checked, int storage, const bp::WindowArgs& a, int dev,
-                  cudaStream_t st) {
+int launch_window(int P, bool checked, int storage, const bp::LaunchArgs& a, bool batch,
+                  long long blocks, int dev, cudaStream_t st) {
   if (storage == BP_STORAGE_F32)
-    return checked ? launch_window_s<MAXRED, true, BP_STORAGE_F32>(P, a, dev, st)
-                   : launch_window_s<MAXRED, false, BP_STORAGE_F32>(P, a, dev, st);
+    return checked ? launch_window_s<MAXRED, true, BP_STORAGE_F32>(P, a, batch, blocks, dev, st)
+                   : launch_window_s<MAXRED, false, BP_STORAGE_F32>(P, a, batch, blocks, dev, st);
   if (checked)
     return fail(BP_ERR_UNSUPPORTED,
                 "non-finite weights in flexible mode need FP32 trace storage");
-  if (storage == BP_STORAGE_BF16) return launch_window_s<MAXRED, false, BP_STORAGE_BF16>(P, a, dev, st);
-  if (storage == BP_STORAGE_F16) return launch_window_s<MAXRED, false, BP_STORAGE_F16>(P, a, dev, st);
+  if (storage == BP_STORAGE_BF16)
+    return launch_window_s<MAXRED, false, BP_STORAGE_BF16>(P, a, batch, blocks, dev, st);
+  if (storage == BP_STORAGE_F16)
+    return launch_window_s<MAXRED, false, BP_STORAGE_F16>(P, a, batch, blocks, dev, st);
   return fail(BP_ERR_INVALID_ARGUMENT, "unknown storage %d", storage);
 }
 
@@ -334,36 +349,48 @@ int check_layout(const bp_table* t, size_t n_samples, size_t lpad, size_t pitch)
   return BP_OK;
 }
 
+bp::TableView table_view(const bp_table* t) {
+  bp::TableView v{};
+  v.src_info = t->dev.src_info;
+  v.tile_hdr = t->dev.tile_hdr;
+  v.st_s = t->dev.st_s;
+  v.st_lo = t->dev.st_lo;
+  v.st_spread = t->dev.st_spread;
+  v.meta = t->dev.meta;
+  v.S = t->dev.S;
+  v.n_tiles = t->dev.n_tiles;
+  return v;
+}
+
 int run_staged(const bp_table* t, const void* traces, int storage, const float* scales,
                size_t T, size_t lpad, size_t pitch, int out_of_bounds, unsigned long long* keys,
                float* beam, size_t ldb, cudaStream_t st) {
-  bp::WindowArgs a{};
-  a.traces = traces;
-  a.scales = scales;
-  a.pitch = (long long)pitch;
-  a.lpad = (int)lpad;
-  a.T = (int)T;
-  a.n_tt = (int)((T + kTimeTile - 1) / kTimeTile);
-  a.n_tiles = t->dev.n_tiles;
-  a.tiles_per_chunk = choose_tiles_per_chunk(a.n_tt, a.n_tiles, t->device);
-  a.S = t->dev.S;
+  bp::LaunchArgs a{};
+  a.tab0 = table_view(t);
+  bp::RecordView& r = a.rec0;
+  r.traces = traces;
+  r.scales = scales;
+  r.pitch = (long long)pitch;
+  r.t_origin = 0;
+  r.lpad = (int)lpad;
+  r.T = (int)T;
+  r.out0 = 0;
+  r.out1 = (int)T;
+  r.flexible = out_of_bounds;
+  r.keys = keys;
+  r.beam = beam;
+  r.ldb = (long long)ldb;
+  const int n_tt = (int)((T + kTimeTile - 1) / kTimeTile);
+  a.tiles_per_chunk = choose_tiles_per_chunk(n_tt, t->dev.n_tiles, t->device);
   a.rowcap = rowcap_for(t);
   a.max_active = std::max(1, t->info.max_active);
-  a.flexible = out_of_bounds;
-  a.src_info = t->dev.src_info;
-  a.tile_hdr = t->dev.tile_hdr;
-  a.st_s = t->dev.st_s;
-  a.st_lo = t->dev.st_lo;
-  a.st_spread = t->dev.st_spread;
-  a.meta = t->dev.meta;
-  a.keys = keys;
-  a.beam = beam;
-  a.ldb = (long long)ldb;
   a.status = t->status;
-  if (a.n_tt == 0) return BP_OK;
+  if (n_tt == 0) return BP_OK;
+  const long long blocks =
+      (long long)((n_tt + a.tiles_per_chunk - 1) / a.tiles_per_chunk) * t->dev.n_tiles;
   const bool checked = out_of_bounds && t->info.any_nonfinite;
-  if (keys) return launch_window<true>(t->dev.P, checked, storage, a, t->device, st);
-  return launch_window<false>(t->dev.P, checked, storage, a, t->device, st);
+  if (keys) return launch_window<true>(t->dev.P, checked, storage, a, false, blocks, t->device, st);
+  return launch_window<false>(t->dev.P, checked, storage, a, false, blocks, t->device, st);
 }
 
 int run_direct(const void* traces, int storage, const float* scales, size_t T, size_t lpad,
@@ -1031,6 +1058,227 @@ int beamform_differential(float* U, int* delays, float* w, size_t T, size_t N, s
     return rc;
   BP_CUDA(cudaMemcpyAsync(beam, d_beam, N * sizeof(float), cudaMemcpyDeviceToHost, st));
   BP_CUDA(cudaStreamSynchronize(st));
+  return BP_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Batches
+// ---------------------------------------------------------------------------
+struct bp_batch {
+  int device;
+  int P;
+  int storage;
+  int n_records;
+  int rowcap;
+  int max_active;
+  bool checked;
+  void* mem;                        // device: tables, records, prefix, keys, srcmm, queue, status
+  bp::TableView* d_tables;
+  bp::RecordView* d_records;
+  long long* d_prefix;
+  unsigned long long* d_keys;
+  size_t n_keys;
+  unsigned long long* d_queue;
+  int* d_status;
+  cudaStream_t stream;
+};
+
+namespace {
+constexpr int kBatchTilesPerItem = 16;  // 4096-sample work items
+
+int masked_minmax(const bp::TableView& tv, int P, const uint32_t* mask, int2* out,
+                  cudaStream_t st) {
+  const long long slots = (long long)tv.n_tiles * kTileSources;
+  const unsigned grid = (unsigned)((slots + 255) / 256);
+  switch (P) {
+    case 1: bp::masked_minmax_kernel<1><<<grid, 256, 0, st>>>(tv, kTileSources, mask, out); break;
+    case 2: bp::masked_minmax_kernel<2><<<grid, 256, 0, st>>>(tv, kTileSources, mask, out); break;
+    case 3: bp::masked_minmax_kernel<3><<<grid, 256, 0, st>>>(tv, kTileSources, mask, out); break;
+    case 4: bp::masked_minmax_kernel<4><<<grid, 256, 0, st>>>(tv, kTileSources, mask, out); break;
+    default: return fail(BP_ERR_UNSUPPORTED, "batches support 1..4 phases");
+  }
+  BP_LAUNCHED("masked_minmax_kernel");
+  return BP_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int bp_batch_create(const bp_table* const* tables, int n_tables, const bp_record* records,
+                    int n_records, int storage, void* stream, bp_batch** out) {
+  g_last_error.clear();
+  if (!out) return fail(BP_ERR_INVALID_ARGUMENT, "out_batch is NULL");
+  *out = nullptr;
+  if (!tables || n_tables <= 0 || !records || n_records <= 0)
+    return fail(BP_ERR_INVALID_ARGUMENT, "empty batch");
+  if (storage != BP_STORAGE_F32 && storage != BP_STORAGE_BF16 && storage != BP_STORAGE_F16)
+    return fail(BP_ERR_INVALID_ARGUMENT, "unknown storage %d", storage);
+  cudaStream_t st = as_stream(stream);
+  int dev = 0;
+  BP_CUDA(cudaGetDevice(&dev));
+  retain_pool(dev);
+  const int P = tables[0] ? tables[0]->dev.P : 0;
+  int rowcap = 0, max_active = 1;
+  bool any_nonfinite = false;
+  std::vector<bp::TableView> tv(n_tables);
+  for (int i = 0; i < n_tables; ++i) {
+    const bp_table* t = tables[i];
+    if (!t) return fail(BP_ERR_INVALID_ARGUMENT, "NULL table %d", i);
+    if (!t->info.uses_window_kernel)
+      return fail(BP_ERR_UNSUPPORTED, "table %d needs the direct kernel; batches use the staged one", i);
+    if (t->dev.P != P) return fail(BP_ERR_INVALID_ARGUMENT, "tables of a batch share n_phases");
+    if (t->device != dev) return fail(BP_ERR_INVALID_ARGUMENT, "table %d is on another device", i);
+    rowcap = std::max(rowcap, rowcap_for(t));
+    max_active = std::max(max_active, t->info.max_active);
+    any_nonfinite |= t->info.any_nonfinite != 0;
+    tv[i] = table_view(t);
+  }
+  std::vector<bp::RecordView> rv(n_records);
+  std::vector<long long> prefix(n_records + 1, 0);
+  size_t n_keys = 0, n_srcmm = 0;
+  bool any_flexible = false;
+  for (int r = 0; r < n_records; ++r) {
+    const bp_record& q = records[r];
+    if (q.table < 0 || q.table >= n_tables)
+      return fail(BP_ERR_INVALID_ARGUMENT, "record %d: table index %d", r, q.table);
+    const bp_table* t = tables[q.table];
+    if (q.out_of_bounds != 0 && q.out_of_bounds != 1)
+      return fail(BP_ERR_INVALID_ARGUMENT, "record %d: out_of_bounds must be 0 or 1", r);
+    if (q.out0 > q.out1 || q.out1 > q.n_samples || q.n_samples > (size_t)kMaxInt / 2)
+      return fail(BP_ERR_INVALID_ARGUMENT, "record %d: output range outside the record", r);
+    if (!q.traces || !q.beam_max || !q.argmax || (storage != BP_STORAGE_F32 && !q.scales))
+      return fail(BP_ERR_INVALID_ARGUMENT, "record %d: NULL pointer", r);
+    if (int rc = check_layout(t, q.n_samples, q.lpad, q.pitch)) return rc;
+    any_flexible |= q.out_of_bounds != 0;
+    bp::RecordView& v = rv[r];
+    v = bp::RecordView{};
+    v.traces = q.traces;
+    v.scales = q.scales;
+    v.pitch = (long long)q.pitch;
+    v.t_origin = q.t_origin;
+    v.lpad = (int)q.lpad;
+    v.T = (int)q.n_samples;
+    v.out0 = (int)q.out0;
+    v.out1 = (int)q.out1;
+    v.flexible = q.out_of_bounds;
+    v.table = q.table;
+    v.tpc = kBatchTilesPerItem;
+    const int tau_first = v.out0 / kTimeTile;
+    const int tau_end = (v.out1 + kTimeTile - 1) / kTimeTile;
+    v.n_chunks = (tau_end - tau_first + v.tpc - 1) / v.tpc;
+    v.station_mask = q.station_mask;
+    v.beam_max = q.beam_max;
+    v.argmax = q.argmax;
+    prefix[r + 1] = prefix[r] + (long long)v.n_chunks * t->dev.n_tiles;
+    n_keys += q.out1 - q.out0;
+    if (q.station_mask) n_srcmm += (size_t)t->dev.n_tiles * kTileSources;
+  }
+  bp_batch* b = new bp_batch();
+  b->device = dev;
+  b->P = P;
+  b->storage = storage;
+  b->n_records = n_records;
+  b->rowcap = rowcap;
+  b->max_active = max_active;
+  b->checked = any_flexible && any_nonfinite;
+  b->stream = st;
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    size_t o = off;
+    off += pad256(std::max<size_t>(bytes, 1));
+    return o;
+  };
+  const size_t o_t = take(n_tables * sizeof(bp::TableView));
+  const size_t o_r = take(n_records * sizeof(bp::RecordView));
+  const size_t o_p = take((n_records + 1) * sizeof(long long));
+  const size_t o_k = take(n_keys * sizeof(unsigned long long));
+  const size_t o_m = take(n_srcmm * sizeof(int2));
+  const size_t o_q = take(sizeof(unsigned long long));
+  const size_t o_s = take(sizeof(int));
+  cudaError_t e = cudaMallocAsync(&b->mem, off, st);
+  if (e != cudaSuccess) {
+    delete b;
+    return cuda_fail(e, "cudaMallocAsync(batch)");
+  }
+  char* base = static_cast<char*>(b->mem);
+  b->d_tables = reinterpret_cast<bp::TableView*>(base + o_t);
+  b->d_records = reinterpret_cast<bp::RecordView*>(base + o_r);
+  b->d_prefix = reinterpret_cast<long long*>(base + o_p);
+  b->d_keys = reinterpret_cast<unsigned long long*>(base + o_k);
+  b->n_keys = n_keys;
+  b->d_queue = reinterpret_cast<unsigned long long*>(base + o_q);
+  b->d_status = reinterpret_cast<int*>(base + o_s);
+  auto bail = [&](int rc) {
+    bp_batch_destroy(b);
+    return rc;
+  };
+  // keys and delay ranges inside the allocation
+  size_t koff = 0, moff = 0;
+  int2* d_srcmm = reinterpret_cast<int2*>(base + o_m);
+  for (int r = 0; r < n_records; ++r) {
+    rv[r].keys = b->d_keys + koff;
+    koff += (size_t)(rv[r].out1 - rv[r].out0);
+    if (records[r].station_mask) {
+      rv[r].srcmm = d_srcmm + moff;
+      const bp::TableView& t = tv[rv[r].table];
+      if (int rc = masked_minmax(t, P, records[r].station_mask, d_srcmm + moff, st))
+        return bail(rc);
+      moff += (size_t)t.n_tiles * kTileSources;
+    }
+  }
+  e = cudaMemcpyAsync(b->d_tables, tv.data(), n_tables * sizeof(bp::TableView),
+                      cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(b->d_records, rv.data(), n_records * sizeof(bp::RecordView),
+                        cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(b->d_prefix, prefix.data(), (n_records + 1) * sizeof(long long),
+                        cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(b->d_status, 0, sizeof(int), st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return bail(cuda_fail(e, "batch descriptors"));
+  *out = b;
+  return BP_OK;
+}
+
+int bp_batch_run(bp_batch* b, void* stream) {
+  g_last_error.clear();
+  if (!b) return fail(BP_ERR_INVALID_ARGUMENT, "NULL batch");
+  cudaStream_t st = as_stream(stream);
+  BP_CUDA(cudaMemsetAsync(b->d_keys, 0, std::max<size_t>(b->n_keys, 1) * 8, st));
+  BP_CUDA(cudaMemsetAsync(b->d_queue, 0, sizeof(unsigned long long), st));
+  bp::LaunchArgs a{};
+  a.tables = b->d_tables;
+  a.records = b->d_records;
+  a.rec_prefix = b->d_prefix;
+  a.n_records = b->n_records;
+  a.next_item = b->d_queue;
+  a.rowcap = b->rowcap;
+  a.max_active = b->max_active;
+  a.status = b->d_status;
+  if (int rc = launch_window<true>(b->P, b->checked, b->storage, a, true, 0, b->device, st))
+    return rc;
+  dim3 grid(64, (unsigned)b->n_records);
+  bp::batch_decode_kernel<<<grid, 256, 0, st>>>(b->d_records);
+  BP_LAUNCHED("batch_decode_kernel");
+  return BP_OK;
+}
+
+int bp_batch_status(bp_batch* b, void* stream, int* status) {
+  if (!b || !status) return fail(BP_ERR_INVALID_ARGUMENT, "NULL argument");
+  cudaStream_t st = as_stream(stream);
+  BP_CUDA(cudaMemcpyAsync(status, b->d_status, sizeof(int), cudaMemcpyDeviceToHost, st));
+  BP_CUDA(cudaStreamSynchronize(st));
+  return BP_OK;
+}
+
+int bp_batch_destroy(bp_batch* b) {
+  if (!b) return BP_OK;
+  if (b->mem) cudaFreeAsync(b->mem, b->stream);
+  cudaStreamSynchronize(b->stream);
+  delete b;
   return BP_OK;
 }
 

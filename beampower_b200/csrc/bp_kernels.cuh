@@ -227,28 +227,52 @@ __global__ void table_build_kernel(const int32_t* __restrict__ delays,
 // warps through shared memory, then one red.global.max.u64 per sample; or,
 // for reduce='none', coalesced stores of the tile's beams.
 // ---------------------------------------------------------------------------
-struct WindowArgs {
-  const void* traces;  // FP32 rows, or 16-bit rows in two versions (see Half16)
-  const float* scales; // per-station scale of 16-bit storage (unused for FP32)
-  long long pitch;     // elements per row
+// A travel-time table as the staged kernel reads it.
+struct TableView {
+  const int4* src_info;  // [n_tiles * K] {source index or -1, min delay, max delay, 0}
+  const int2* tile_hdr;  // [n_tiles] {active stations, 0}
+  const int* st_s;       // [n_tiles * S]
+  const int* st_lo;      // [n_tiles * S * P]
+  const int* st_spread;  // [n_tiles * S * P]
+  const void* meta;      // [n_tiles * S * K]
+  int S, n_tiles;
+};
+
+// One record: a waveform window, or a streamed chunk with its carried halo.
+// Sample t of the record is global sample t_origin + t.  Traces hold samples
+// [0, T) (zeros outside); results are produced for samples [out0, out1).
+struct RecordView {
+  const void* traces;   // FP32 rows, or 16-bit rows in two versions (see Half16)
+  const float* scales;  // per-station scale of 16-bit storage (unused for FP32)
+  long long pitch;      // elements per row
+  long long t_origin;   // global index of record sample 0 (strict lower bound)
   int lpad;
   int T;
-  int n_tt;            // time tiles covering T
-  int tiles_per_chunk; // time tiles per block
-  int n_tiles;
-  int S;
-  int rowcap;          // elements per ring row (per version for 16-bit)
-  int max_active;
+  int out0, out1;
   int flexible;
-  const int4* src_info;
-  const int2* tile_hdr;
-  const int* st_s;
-  const int* st_lo;
-  const int* st_spread;
-  const void* meta;
-  unsigned long long* keys;
-  float* beam;
+  int table;                    // index into the launch's tables
+  int tpc;                      // batch launch: time tiles per work item
+  int n_chunks;                 // batch launch: work items per source tile
+  const uint32_t* station_mask; // bit s set: station s used (nullptr: all)
+  const int2* srcmm;            // per tile slot (min, max) over used stations, or nullptr
+  unsigned long long* keys;     // [out1 - out0] packed keys (reduce='max')
+  float* beam;                  // [N, ldb], column = sample - out0 (reduce='none')
   long long ldb;
+  float* beam_max;              // batch launch: decoded outputs [out1 - out0]
+  int32_t* argmax;
+};
+
+struct LaunchArgs {
+  TableView tab0;               // plain launch: the table
+  RecordView rec0;              // plain launch: the record
+  const TableView* tables;      // batch launch: device arrays
+  const RecordView* records;
+  const long long* rec_prefix;  // batch launch: work items before record r, [n_records + 1]
+  int n_records;
+  unsigned long long* next_item;  // batch launch: work-queue head
+  int tiles_per_chunk;          // plain launch: time tiles per block
+  int rowcap;                   // elements per ring row (per version for 16-bit)
+  int max_active;
   int* status;
 };
 
@@ -269,7 +293,7 @@ struct WindowSmem {
   using M = typename MetaT<P>::type;
   static constexpr int K = WS * KS;
   static constexpr int TT = 32 * MT;
-  size_t ring, meta, red, srci, st_s, st_lo, st_w, st_sc, bars, abort_flag, total;
+  size_t ring, meta, red, srci, st_s, st_lo, st_w, st_sc, bars, misc, total;
   __host__ __device__ WindowSmem(int rowcap, int max_active) {
     size_t o = 0;
     ring = o;        o += (size_t)NSTAGE * P * rowcap * 4;
@@ -285,37 +309,10 @@ struct WindowSmem {
     st_sc = o;       o += (size_t)max_active * sizeof(float);
     o = align_up_sz(o, 8);
     bars = o;        o += (size_t)2 * NSTAGE * sizeof(uint64_t);
-    abort_flag = o;  o += 16;
+    misc = o;        o += 64;  // abort flag, active count, current item
     total = align_up_sz(o, 128);
   }
 };
-
-// 16-bit pair (low half = earlier sample) -> FP32 pair, and FP32 += pair.
-template <int STORAGE>
-__device__ __forceinline__ float2 h16x2_cvt(uint32_t w) {
-  float2 r;
-  if constexpr (STORAGE == BP_STORAGE_BF16)
-    asm("{\n\t.reg .b16 lo, hi;\n\tmov.b32 {lo, hi}, %2;\n\t"
-        "cvt.f32.bf16 %0, lo;\n\tcvt.f32.bf16 %1, hi;\n\t}"
-        : "=f"(r.x), "=f"(r.y) : "r"(w));
-  else
-    asm("{\n\t.reg .b16 lo, hi;\n\tmov.b32 {lo, hi}, %2;\n\t"
-        "cvt.f32.f16 %0, lo;\n\tcvt.f32.f16 %1, hi;\n\t}"
-        : "=f"(r.x), "=f"(r.y) : "r"(w));
-  return r;
-}
-
-template <int STORAGE>
-__device__ __forceinline__ void h16x2_add(float2& acc, uint32_t w) {
-  if constexpr (STORAGE == BP_STORAGE_BF16)
-    asm("{\n\t.reg .b16 lo, hi;\n\tmov.b32 {lo, hi}, %2;\n\t"
-        "add.rn.f32.bf16 %0, lo, %0;\n\tadd.rn.f32.bf16 %1, hi, %1;\n\t}"
-        : "+f"(acc.x), "+f"(acc.y) : "r"(w));
-  else
-    asm("{\n\t.reg .b16 lo, hi;\n\tmov.b32 {lo, hi}, %2;\n\t"
-        "add.rn.f32.f16 %0, lo, %0;\n\tadd.rn.f32.f16 %1, hi, %1;\n\t}"
-        : "+f"(acc.x), "+f"(acc.y) : "r"(w));
-}
 
 // Sample of accumulator half h of pair q for this lane, relative to t0.
 // FP32: lane owns samples lane + 32 m (pair q = m 2q, 2q+1);
@@ -330,312 +327,494 @@ __device__ __forceinline__ int pair_sample(int lane, int q, int h) {
 #define BP_WINDOW_MIN_BLOCKS 2
 #endif
 
+// The staged shift-and-stack for one item (record, source tile, time tiles
+// [tau0, tau1)), shared by the plain and the persistent kernels.
 template <int P, int KS, int MT, int WS, int NSTAGE, bool MAXRED, bool CHECKED, int STORAGE>
-__global__ void __launch_bounds__((WS + 1) * 32, BP_WINDOW_MIN_BLOCKS)
-beam_window_kernel(const WindowArgs a) {
+struct Staged {
   static_assert(MT % 2 == 0 && KS % 2 == 0, "packed pairs");
   static_assert(!(CHECKED && STORAGE != BP_STORAGE_F32), "checked variant is FP32 only");
   using M = typename MetaT<P>::type;
-  constexpr bool F32 = STORAGE == BP_STORAGE_F32;
-  constexpr int K = WS * KS;
-  constexpr int TT = 32 * MT;
-  constexpr int NCONS = WS * 32;
-  constexpr int ESZ = F32 ? 4 : 2;  // bytes per stored element
-  constexpr int NVER = F32 ? 1 : 2; // stored versions per row
-  extern __shared__ __align__(128) unsigned char smem[];
-  const WindowSmem<P, KS, MT, WS, NSTAGE, MAXRED> L(a.rowcap, a.max_active);
-  unsigned char* ring = smem + L.ring;
-  M* meta_s = reinterpret_cast<M*>(smem + L.meta);
-  unsigned long long* red = reinterpret_cast<unsigned long long*>(smem + L.red);
-  int4* srci = reinterpret_cast<int4*>(smem + L.srci);
-  int* st_s = reinterpret_cast<int*>(smem + L.st_s);
-  int* st_lo = reinterpret_cast<int*>(smem + L.st_lo);
-  int* st_w = reinterpret_cast<int*>(smem + L.st_w);
-  float* st_sc = reinterpret_cast<float*>(smem + L.st_sc);
-  uint64_t* full = reinterpret_cast<uint64_t*>(smem + L.bars);
-  uint64_t* empty = full + NSTAGE;
-  volatile int* abort_flag = reinterpret_cast<volatile int*>(smem + L.abort_flag);
-  const size_t row_bytes = (size_t)a.rowcap * 4;  // one ring row (all versions)
+  static constexpr bool F32 = STORAGE == BP_STORAGE_F32;
+  static constexpr int K = WS * KS;
+  static constexpr int TT = 32 * MT;
+  static constexpr int NCONS = WS * 32;
+  static constexpr int ESZ = F32 ? 4 : 2;  // bytes per stored element
+  static constexpr int NVER = F32 ? 1 : 2; // stored versions per row
 
-  const int tile = blockIdx.x % a.n_tiles;
-  const int chunk = blockIdx.x / a.n_tiles;
-  const int tau0 = chunk * a.tiles_per_chunk;
-  const int tau1 = min(tau0 + a.tiles_per_chunk, a.n_tt);
-  const int tid = threadIdx.x;
-  const int warp = tid >> 5;
-  const int lane = tid & 31;
-  const int n_active = a.tile_hdr[tile].x;
+  struct Smem {
+    unsigned char* ring;
+    M* meta_s;
+    unsigned long long* red;
+    int4* srci;
+    int* st_s;
+    int* st_lo;
+    int* st_w;
+    float* st_sc;
+    uint64_t* full;
+    uint64_t* empty;
+    volatile int* abort_flag;
+    int* n_act;
+    int4* cur_item;
+  };
 
-  // ---- prologue: the tile's metadata into shared memory -----------------
-  {
-    const M* gm = reinterpret_cast<const M*>(a.meta) + (size_t)tile * a.S * K;
-    if constexpr (F32) {
-      for (int i = tid; i < n_active * K; i += blockDim.x) meta_s[i] = gm[i];
-    } else {
-      // 16-bit: turn each sample offset into the 32-bit word offset inside
-      // the ring row, version included: (off >> 1) + (off & 1) * rowcap / 2
-      // (version 1 starts rowcap / 2 words into the row).
-      const uint32_t half_row = (uint32_t)a.rowcap >> 1;
+  __device__ static Smem carve(unsigned char* smem, int rowcap, int max_active) {
+    const WindowSmem<P, KS, MT, WS, NSTAGE, MAXRED> L(rowcap, max_active);
+    Smem s;
+    s.ring = smem + L.ring;
+    s.meta_s = reinterpret_cast<M*>(smem + L.meta);
+    s.red = reinterpret_cast<unsigned long long*>(smem + L.red);
+    s.srci = reinterpret_cast<int4*>(smem + L.srci);
+    s.st_s = reinterpret_cast<int*>(smem + L.st_s);
+    s.st_lo = reinterpret_cast<int*>(smem + L.st_lo);
+    s.st_w = reinterpret_cast<int*>(smem + L.st_w);
+    s.st_sc = reinterpret_cast<float*>(smem + L.st_sc);
+    s.full = reinterpret_cast<uint64_t*>(smem + L.bars);
+    s.empty = s.full + NSTAGE;
+    s.abort_flag = reinterpret_cast<volatile int*>(smem + L.misc);
+    s.n_act = reinterpret_cast<int*>(smem + L.misc + 16);
+    s.cur_item = reinterpret_cast<int4*>(smem + L.misc + 32);
+    return s;
+  }
+
+  // thread 0, once per block
+  __device__ static void init_barriers(const Smem& sm) {
+    for (int s = 0; s < NSTAGE; ++s) {
+      mbar_init(&sm.full[s], 1);
+      mbar_init(&sm.empty[s], WS);
+    }
+    *sm.abort_flag = 0;
+    fence_mbar_init();
+  }
+
+  // All threads.  Ends after the item's last epilogue; the caller puts a
+  // __syncthreads() between items.  `it0` is the block's stage counter
+  // before the item; returns the number of stages the item used.
+  __device__ static int run_item(const Smem& sm, const TableView& tb, const RecordView& rc,
+                                 int tile, int tau0, int tau1, int rowcap, int* status,
+                                 int it0) {
+    const int tid = threadIdx.x;
+    const int warp = tid >> 5;
+    const int lane = tid & 31;
+    const int row_words = rowcap;  // one ring row (all versions) in 32-bit words
+
+    // ---- prologue: the tile's stations (those the record uses) ----------
+    if (warp == 0) {
+      const int n_tab = tb.tile_hdr[tile].x;
+      int n = 0;
+      for (int j0 = 0; j0 < n_tab; j0 += 32) {
+        const int j = j0 + lane;
+        int s = -1;
+        bool use = false;
+        if (j < n_tab) {
+          s = tb.st_s[(size_t)tile * tb.S + j];
+          use = !rc.station_mask || ((rc.station_mask[s >> 5] >> (s & 31)) & 1u);
+        }
+        const unsigned bal = __ballot_sync(0xFFFFFFFFu, use);
+        if (use) {
+          const int jj = n + __popc(bal & ((1u << lane) - 1u));
+          sm.st_s[jj] = j;  // table slot for now; station index filled below
+        }
+        n += __popc(bal);
+      }
+      if (lane == 0) *sm.n_act = n;
+    }
+    __syncthreads();
+    const int n_active = *sm.n_act;
+    {
+      const M* gm = reinterpret_cast<const M*>(tb.meta) + (size_t)tile * tb.S * K;
+      const uint32_t half_row = (uint32_t)rowcap >> 1;
       for (int i = tid; i < n_active * K; i += blockDim.x) {
-        M m = gm[i];
-        auto wo = [&](uint32_t v) {
-          const uint32_t lo = v & 0xFFFFu, hi = v >> 16;
-          return ((lo >> 1) + (lo & 1u) * half_row) | (((hi >> 1) + (hi & 1u) * half_row) << 16);
-        };
-        m.y = wo(m.y);
-        if constexpr (P > 2) m.z = wo(m.z);
-        meta_s[i] = m;
+        const int jj = i / K, k = i - jj * K;
+        M m = gm[(size_t)sm.st_s[jj] * K + k];
+        if constexpr (!F32) {
+          // 16-bit: each sample offset becomes the 32-bit word offset in
+          // the ring row, version included: (off >> 1) + (off & 1) * rowcap / 2
+          // (version 1 starts rowcap / 2 words into the row).
+          auto wo = [&](uint32_t v) {
+            const uint32_t lo = v & 0xFFFFu, hi = v >> 16;
+            return ((lo >> 1) + (lo & 1u) * half_row) |
+                   (((hi >> 1) + (hi & 1u) * half_row) << 16);
+          };
+          m.y = wo(m.y);
+          if constexpr (P > 2) m.z = wo(m.z);
+        }
+        sm.meta_s[i] = m;
+      }
+      for (int i = tid; i < K; i += blockDim.x) {
+        int4 si = tb.src_info[(size_t)tile * K + i];
+        if (rc.srcmm) {
+          const int2 mm = rc.srcmm[(size_t)tile * K + i];
+          si.y = mm.x;
+          si.z = mm.y;
+        }
+        sm.srci[i] = si;
       }
     }
-    for (int i = tid; i < K; i += blockDim.x) srci[i] = a.src_info[(size_t)tile * K + i];
+    __syncthreads();  // the meta copy above read st_s[] as table slots
     for (int i = tid; i < n_active; i += blockDim.x) {
-      const int s = a.st_s[(size_t)tile * a.S + i];
-      st_s[i] = s;
-      st_sc[i] = F32 ? 1.0f : a.scales[s];
+      // entry i is read and rewritten by this thread only
+      const int j = sm.st_s[i];
+      const int s = tb.st_s[(size_t)tile * tb.S + j];
+      sm.st_s[i] = s;
+      sm.st_sc[i] = F32 ? 1.0f : rc.scales[s];
 #pragma unroll
       for (int p = 0; p < P; ++p) {
-        const size_t g = ((size_t)tile * a.S + i) * P + p;
-        st_lo[i * P + p] = a.st_lo[g];
-        const int w = (int)align_up_sz((size_t)(TT + a.st_spread[g] + 1), kAlign);
-        st_w[i * P + p] = w;
-        if (w > a.rowcap) atomicOr(a.status, kStatusBadWindow);
+        const size_t g = ((size_t)tile * tb.S + j) * P + p;
+        sm.st_lo[i * P + p] = tb.st_lo[g];
+        const int w = (int)align_up_sz((size_t)(TT + tb.st_spread[g] + 1), kAlign);
+        sm.st_w[i * P + p] = w;
+        if (w > rowcap) atomicOr(status, kStatusBadWindow);
       }
     }
-    if (tid == 0) {
-      for (int s = 0; s < NSTAGE; ++s) {
-        mbar_init(&full[s], 1);
-        mbar_init(&empty[s], WS);
+    __syncthreads();
+
+    const int n_stages = (tau1 - tau0) * n_active;
+
+    // ---- producer warp ----------------------------------------------------
+    if (warp == WS) {
+      if (lane == 0) {
+        const unsigned char* tr = reinterpret_cast<const unsigned char*>(rc.traces);
+        int issued = 0;
+        for (int r = 0; r < n_stages; ++r) {
+          const int it = it0 + r;
+          const int stage = it % NSTAGE;
+          if (it >= NSTAGE && !mbar_wait_bounded(&sm.empty[stage], ((it / NSTAGE) - 1) & 1,
+                                                 sm.abort_flag, status))
+            break;
+          const int tau = tau0 + r / n_active;
+          const int j = r - (r / n_active) * n_active;
+          const int t0 = tau * TT;
+          const int s = sm.st_s[j];
+          uint32_t bytes = 0;
+#pragma unroll
+          for (int p = 0; p < P; ++p)
+            bytes += (uint32_t)min(sm.st_w[j * P + p], rowcap) * ESZ * NVER;
+          mbar_arrive_expect_tx(&sm.full[stage], bytes);
+#pragma unroll
+          for (int p = 0; p < P; ++p) {
+            const int w = min(sm.st_w[j * P + p], rowcap);
+            const long long col = (long long)rc.lpad + t0 + sm.st_lo[j * P + p];
+#pragma unroll
+            for (int v = 0; v < NVER; ++v) {
+              const size_t row = (size_t)(s * P + p) * NVER + v;
+              bulk_g2s(sm.ring + ((size_t)(stage * P + p) * row_words) * 4 +
+                           (size_t)v * rowcap * ESZ,
+                       tr + (row * rc.pitch + col) * ESZ, (uint32_t)w * ESZ, &sm.full[stage]);
+            }
+          }
+          ++issued;
+        }
+        if (*sm.abort_flag) {
+          // Let every copy already issued land before the block moves on.
+          volatile int never = 0;
+          for (int r = max(0, issued - NSTAGE); r < issued; ++r) {
+            const int it = it0 + r;
+            mbar_wait_bounded(&sm.full[it % NSTAGE], (it / NSTAGE) & 1, &never, nullptr);
+          }
+        }
       }
-      *abort_flag = 0;
-      fence_mbar_init();
+      return n_stages;
     }
-  }
-  __syncthreads();
 
-  const int n_items = (tau1 - tau0) * n_active;
+    // ---- consumer warps ---------------------------------------------------
+    const int4* my_src = sm.srci + warp * KS;
+    int it = it0;
+    for (int tau = tau0; tau < tau1; ++tau) {
+      float2 acc[KS][MT / 2];  // pair q, half h: sample pair_sample(lane, q, h)
+#pragma unroll
+      for (int k = 0; k < KS; ++k)
+#pragma unroll
+        for (int m = 0; m < MT / 2; ++m) acc[k][m] = make_float2(0.0f, 0.0f);
+      const int t0 = tau * TT;
 
-  // ---- producer warp ------------------------------------------------------
-  if (warp == WS) {
-    if (lane == 0) {
-      const unsigned char* tr = reinterpret_cast<const unsigned char*>(a.traces);
-      int issued = 0;
-      for (int it = 0; it < n_items; ++it) {
+      for (int j = 0; j < n_active; ++j, ++it) {
         const int stage = it % NSTAGE;
-        if (it >= NSTAGE &&
-            !mbar_wait_bounded(&empty[stage], ((it / NSTAGE) - 1) & 1, abort_flag, a.status))
-          break;
-        const int tau = tau0 + it / n_active;
-        const int j = it - (it / n_active) * n_active;
-        const int t0 = tau * TT;
-        const int s = st_s[j];
-        uint32_t bytes = 0;
+        mbar_wait_bounded(&sm.full[stage], (it / NSTAGE) & 1, sm.abort_flag, status);
+        // stage base in 32-bit words; row p of the stage at + p * rowcap words
+        const int sbase = stage * P * row_words;
+        const M* mrow = sm.meta_s + (size_t)j * K + warp * KS;
+        const float scale = sm.st_sc[j];
 #pragma unroll
-        for (int p = 0; p < P; ++p) bytes += (uint32_t)min(st_w[j * P + p], a.rowcap) * ESZ * NVER;
-        mbar_arrive_expect_tx(&full[stage], bytes);
-#pragma unroll
-        for (int p = 0; p < P; ++p) {
-          const int w = min(st_w[j * P + p], a.rowcap);
-          const long long col = (long long)a.lpad + t0 + st_lo[j * P + p];
-#pragma unroll
-          for (int v = 0; v < NVER; ++v) {
-            const size_t row = (size_t)(s * P + p) * NVER + v;
-            bulk_g2s(ring + (size_t)(stage * P + p) * row_bytes + (size_t)v * a.rowcap * ESZ,
-                     tr + (row * a.pitch + col) * ESZ, (uint32_t)w * ESZ, &full[stage]);
-          }
-        }
-        ++issued;
-      }
-      if (*abort_flag) {
-        // Let every copy already issued land before the block can exit.
-        volatile int never = 0;
-        for (int it = max(0, issued - NSTAGE); it < issued; ++it)
-          mbar_wait_bounded(&full[it % NSTAGE], (it / NSTAGE) & 1, &never, nullptr);
-      }
-    }
-    return;
-  }
-
-  // ---- consumer warps -----------------------------------------------------
-  const int4* my_src = srci + warp * KS;
-  int it = 0;
-  for (int tau = tau0; tau < tau1; ++tau) {
-    float2 acc[KS][MT / 2];  // pair q, half h: sample pair_sample(lane, q, h)
-#pragma unroll
-    for (int k = 0; k < KS; ++k)
-#pragma unroll
-      for (int m = 0; m < MT / 2; ++m) acc[k][m] = make_float2(0.0f, 0.0f);
-    const int t0 = tau * TT;
-
-    for (int j = 0; j < n_active; ++j, ++it) {
-      const int stage = it % NSTAGE;
-      mbar_wait_bounded(&full[stage], (it / NSTAGE) & 1, abort_flag, a.status);
-      // stage base in 32-bit words; row p of the stage at + p * rowcap words
-      const int sbase = stage * P * a.rowcap;
-      const M* mrow = meta_s + (size_t)j * K + warp * KS;
-      const float scale = st_sc[j];
-#pragma unroll
-      for (int k2 = 0; k2 < KS; k2 += 2) {
-        M mm2[2];
-        if constexpr (P <= 2) {
-          // two sources' records in one 128-bit broadcast
-          const uint4 q4 = *reinterpret_cast<const uint4*>(mrow + k2);
-          mm2[0] = make_uint2(q4.x, q4.y);
-          mm2[1] = make_uint2(q4.z, q4.w);
-        } else {
-          mm2[0] = mrow[k2];
-          mm2[1] = mrow[k2 + 1];
-        }
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          const int k = k2 + h;
-          const M m = mm2[h];
-          const float w = __uint_as_float(m.x);
-          if (w == 0.0f) continue;  // warp-uniform: skipped station
-          if constexpr (!F32) {
-            // 16-bit: sum the phases in FP32, then one fused multiply-add
-            // per sample pair with c = w * scale (exact: scale is 2^k).
-            const float c = w * scale;
-            const float2 c2 = make_float2(c, c);
-            const uint32_t* src[P];  // word offsets prepared in the prologue
-#pragma unroll
-            for (int p = 0; p < P; ++p)
-              src[p] = reinterpret_cast<const uint32_t*>(ring) + sbase + p * a.rowcap +
-                       meta_off<P>(m, p) + lane;
-            uint32_t wd[P][MT / 2];  // all words first (see the FP32 path)
-#pragma unroll
-            for (int p = 0; p < P; ++p)
-#pragma unroll
-              for (int q = 0; q < MT / 2; ++q) wd[p][q] = src[p][32 * q];
-#pragma unroll
-            for (int q = 0; q < MT / 2; ++q) {
-              float2 ps;
-              if constexpr (STORAGE == BP_STORAGE_F16) {
-                // phases summed in FP16 pairs (one extra FP16 rounding of a
-                // sum of values in [-P, P]), then widened once
-                __half2 hs = *reinterpret_cast<const __half2*>(&wd[0][q]);
-#pragma unroll
-                for (int p = 1; p < P; ++p)
-                  hs = __hadd2(hs, *reinterpret_cast<const __half2*>(&wd[p][q]));
-                ps = __half22float2(hs);
-              } else {
-                // BF16 -> FP32 is exact bit placement; phases summed in FP32
-                ps = make_float2(__uint_as_float(wd[0][q] << 16),
-                                 __uint_as_float(wd[0][q] & 0xFFFF0000u));
-#pragma unroll
-                for (int p = 1; p < P; ++p)
-                  ps = add2_rn(ps, make_float2(__uint_as_float(wd[p][q] << 16),
-                                               __uint_as_float(wd[p][q] & 0xFFFF0000u)));
-              }
-              acc[k][q] = __ffma2_rn(c2, ps, acc[k][q]);
-            }
-          } else if constexpr (CHECKED) {
-#pragma unroll
-            for (int p = 0; p < P; ++p) {
-              const int off = meta_off<P>(m, p);
-              const float* src =
-                  reinterpret_cast<const float*>(ring) + sbase + p * a.rowcap + off + lane;
-              const long long tb = (long long)t0 + lane + st_lo[j * P + p] + off;
-#pragma unroll
-              for (int mm = 0; mm < MT; ++mm) {
-                const long long tt = tb + 32 * mm;
-                if (tt < 0 || tt >= a.T) continue;
-                const float v = __fadd_rn((mm & 1) ? acc[k][mm >> 1].y : acc[k][mm >> 1].x,
-                                          __fmul_rn(w, src[mm * 32]));
-                if (mm & 1) acc[k][mm >> 1].y = v; else acc[k][mm >> 1].x = v;
-              }
-            }
+        for (int k2 = 0; k2 < KS; k2 += 2) {
+          M mm2[2];
+          if constexpr (P <= 2) {
+            // two sources' records in one 128-bit broadcast
+            const uint4 q4 = *reinterpret_cast<const uint4*>(mrow + k2);
+            mm2[0] = make_uint2(q4.x, q4.y);
+            mm2[1] = make_uint2(q4.z, q4.w);
           } else {
-            // All of this source's words first, then the arithmetic: the
-            // loads of one (source, station) are independent, and issuing
-            // them together keeps P * MT shared-memory loads in flight.
-            const float* sbf = reinterpret_cast<const float*>(ring) + sbase + lane;
-            float u[P][MT];
+            mm2[0] = mrow[k2];
+            mm2[1] = mrow[k2 + 1];
+          }
 #pragma unroll
-            for (int p = 0; p < P; ++p) {
-              const float* src = sbf + p * a.rowcap + meta_off<P>(m, p);
+          for (int h = 0; h < 2; ++h) {
+            const int k = k2 + h;
+            const M m = mm2[h];
+            const float w = __uint_as_float(m.x);
+            if (w == 0.0f) continue;  // warp-uniform: skipped station
+            if constexpr (!F32) {
+              // 16-bit: sum the phases, then one fused multiply-add per
+              // sample pair with c = w * scale (exact: scale is 2^k).
+              const float c = w * scale;
+              const float2 c2 = make_float2(c, c);
+              const uint32_t* src[P];  // word offsets prepared in the prologue
 #pragma unroll
-              for (int mm = 0; mm < MT; ++mm) u[p][mm] = src[32 * mm];
-            }
-            if (w == 1.0f) {  // warp-uniform: 1 * u == u exactly, skip the multiply
+              for (int p = 0; p < P; ++p)
+                src[p] = reinterpret_cast<const uint32_t*>(sm.ring) + sbase + p * row_words +
+                         meta_off<P>(m, p) + lane;
+              uint32_t wd[P][MT / 2];  // all words first (see the FP32 path)
 #pragma unroll
               for (int p = 0; p < P; ++p)
 #pragma unroll
-                for (int q = 0; q < MT / 2; ++q)
-                  acc[k][q] = add2_rn(acc[k][q], make_float2(u[p][2 * q], u[p][2 * q + 1]));
-            } else {
-              // Scalar rounded multiply then rounded add: a packed multiply
-              // followed by a packed add can be fused downstream, which would
-              // change the last bit against the reference.
+                for (int q = 0; q < MT / 2; ++q) wd[p][q] = src[p][32 * q];
 #pragma unroll
-              for (int p = 0; p < P; ++p)
+              for (int q = 0; q < MT / 2; ++q) {
+                float2 ps;
+                if constexpr (STORAGE == BP_STORAGE_F16) {
+                  // phases summed in FP16 pairs (one extra FP16 rounding of a
+                  // sum of values in [-P, P]), then widened once
+                  __half2 hs = *reinterpret_cast<const __half2*>(&wd[0][q]);
 #pragma unroll
-                for (int q = 0; q < MT / 2; ++q) {
-                  acc[k][q].x = __fadd_rn(acc[k][q].x, __fmul_rn(w, u[p][2 * q]));
-                  acc[k][q].y = __fadd_rn(acc[k][q].y, __fmul_rn(w, u[p][2 * q + 1]));
+                  for (int p = 1; p < P; ++p)
+                    hs = __hadd2(hs, *reinterpret_cast<const __half2*>(&wd[p][q]));
+                  ps = __half22float2(hs);
+                } else {
+                  // BF16 -> FP32 is exact bit placement; phases summed in FP32
+                  ps = make_float2(__uint_as_float(wd[0][q] << 16),
+                                   __uint_as_float(wd[0][q] & 0xFFFF0000u));
+#pragma unroll
+                  for (int p = 1; p < P; ++p)
+                    ps = add2_rn(ps, make_float2(__uint_as_float(wd[p][q] << 16),
+                                                 __uint_as_float(wd[p][q] & 0xFFFF0000u)));
                 }
+                acc[k][q] = __ffma2_rn(c2, ps, acc[k][q]);
+              }
+            } else if constexpr (CHECKED) {
+#pragma unroll
+              for (int p = 0; p < P; ++p) {
+                const int off = meta_off<P>(m, p);
+                const float* src = reinterpret_cast<const float*>(sm.ring) + sbase +
+                                   p * row_words + off + lane;
+                const long long tb0 = (long long)t0 + lane + sm.st_lo[j * P + p] + off;
+#pragma unroll
+                for (int mm = 0; mm < MT; ++mm) {
+                  const long long tt = tb0 + 32 * mm;
+                  if (tt < 0 || tt >= rc.T) continue;
+                  const float v = __fadd_rn((mm & 1) ? acc[k][mm >> 1].y : acc[k][mm >> 1].x,
+                                            __fmul_rn(w, src[mm * 32]));
+                  if (mm & 1) acc[k][mm >> 1].y = v; else acc[k][mm >> 1].x = v;
+                }
+              }
+            } else {
+              // All of this source's words first, then the arithmetic: the
+              // loads of one (source, station) are independent, and issuing
+              // them together keeps P * MT shared-memory loads in flight.
+              const float* sbf = reinterpret_cast<const float*>(sm.ring) + sbase + lane;
+              float u[P][MT];
+#pragma unroll
+              for (int p = 0; p < P; ++p) {
+                const float* src = sbf + p * row_words + meta_off<P>(m, p);
+#pragma unroll
+                for (int mm = 0; mm < MT; ++mm) u[p][mm] = src[32 * mm];
+              }
+              if (w == 1.0f) {  // warp-uniform: 1 * u == u exactly, skip the multiply
+#pragma unroll
+                for (int p = 0; p < P; ++p)
+#pragma unroll
+                  for (int q = 0; q < MT / 2; ++q)
+                    acc[k][q] = add2_rn(acc[k][q], make_float2(u[p][2 * q], u[p][2 * q + 1]));
+              } else {
+                // Scalar rounded multiply then rounded add: a packed multiply
+                // followed by a packed add can be fused downstream, which would
+                // change the last bit against the reference.
+#pragma unroll
+                for (int p = 0; p < P; ++p)
+#pragma unroll
+                  for (int q = 0; q < MT / 2; ++q) {
+                    acc[k][q].x = __fadd_rn(acc[k][q].x, __fmul_rn(w, u[p][2 * q]));
+                    acc[k][q].y = __fadd_rn(acc[k][q].y, __fmul_rn(w, u[p][2 * q + 1]));
+                  }
+              }
             }
           }
         }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&sm.empty[stage]);
       }
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&empty[stage]);
-    }
 
-    // ---- epilogue of the time tile ----
-    if constexpr (MAXRED) {
-#pragma unroll
-      for (int q = 0; q < MT / 2; ++q) {
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          const int rel = pair_sample<STORAGE>(lane, q, h);
-          const long long t = (long long)t0 + rel;
-          unsigned long long best = 0ull;
-#pragma unroll
-          for (int k = 0; k < KS; ++k) {
-            const int4 si = my_src[k];
-            if (si.x < 0) continue;
-            const bool valid =
-                a.flexible ? true
-                           : (si.y <= si.z && t + si.y >= 0 && t + (long long)si.z < a.T);
-            if (!valid) continue;
-            const unsigned long long key = make_key(h ? acc[k][q].y : acc[k][q].x, si.x);
-            best = key > best ? key : best;
-          }
-          red[warp * TT + rel] = best;
-        }
-      }
-      named_barrier_sync(1, NCONS);
-      for (int i = tid; i < TT; i += NCONS) {
-        unsigned long long best = 0ull;
-#pragma unroll
-        for (int w = 0; w < WS; ++w) {
-          const unsigned long long v = red[w * TT + i];
-          best = v > best ? v : best;
-        }
-        if (best != 0ull && t0 + i < a.T) red_max_u64(&a.keys[t0 + i], best);
-      }
-      named_barrier_sync(1, NCONS);
-    } else {
-#pragma unroll
-      for (int k = 0; k < KS; ++k) {
-        const int4 si = my_src[k];
-        if (si.x < 0) continue;
-        float* row = a.beam + (size_t)si.x * a.ldb;
+      // ---- epilogue of the time tile ----
+      if constexpr (MAXRED) {
 #pragma unroll
         for (int q = 0; q < MT / 2; ++q) {
 #pragma unroll
           for (int h = 0; h < 2; ++h) {
-            const long long t = (long long)t0 + pair_sample<STORAGE>(lane, q, h);
-            if (t >= a.T) continue;
-            const bool valid =
-                a.flexible ? true
-                           : (si.y <= si.z && t + si.y >= 0 && t + (long long)si.z < a.T);
-            if (valid) row[t] = h ? acc[k][q].y : acc[k][q].x;
+            const int rel = pair_sample<STORAGE>(lane, q, h);
+            const long long t = (long long)t0 + rel;
+            const long long g = rc.t_origin + t;
+            unsigned long long best = 0ull;
+#pragma unroll
+            for (int k = 0; k < KS; ++k) {
+              const int4 si = my_src[k];
+              if (si.x < 0) continue;
+              const bool valid =
+                  rc.flexible ? true
+                              : (si.y <= si.z && g + si.y >= 0 && t + (long long)si.z < rc.T);
+              if (!valid) continue;
+              const unsigned long long key = make_key(h ? acc[k][q].y : acc[k][q].x, si.x);
+              best = key > best ? key : best;
+            }
+            sm.red[warp * TT + rel] = best;
+          }
+        }
+        named_barrier_sync(1, NCONS);
+        for (int i = tid; i < TT; i += NCONS) {
+          unsigned long long best = 0ull;
+#pragma unroll
+          for (int w = 0; w < WS; ++w) {
+            const unsigned long long v = sm.red[w * TT + i];
+            best = v > best ? v : best;
+          }
+          const int t = t0 + i;
+          if (best != 0ull && t >= rc.out0 && t < rc.out1) red_max_u64(&rc.keys[t - rc.out0], best);
+        }
+        named_barrier_sync(1, NCONS);
+      } else {
+#pragma unroll
+        for (int k = 0; k < KS; ++k) {
+          const int4 si = my_src[k];
+          if (si.x < 0) continue;
+          float* row = rc.beam + (size_t)si.x * rc.ldb - rc.out0;
+#pragma unroll
+          for (int q = 0; q < MT / 2; ++q) {
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+              const long long t = (long long)t0 + pair_sample<STORAGE>(lane, q, h);
+              if (t < rc.out0 || t >= rc.out1) continue;
+              const long long g = rc.t_origin + t;
+              const bool valid =
+                  rc.flexible ? true
+                              : (si.y <= si.z && g + si.y >= 0 && t + (long long)si.z < rc.T);
+              if (valid) row[t] = h ? acc[k][q].y : acc[k][q].x;
+            }
           }
         }
       }
     }
+    return n_stages;
   }
+};
+
+// Plain launch: one record, block = (source tile, chunk of time tiles),
+// time-chunk major so that the blocks in flight share an L2-resident stretch
+// of trace.
+template <int P, int KS, int MT, int WS, int NSTAGE, bool MAXRED, bool CHECKED, int STORAGE>
+__global__ void __launch_bounds__((WS + 1) * 32, BP_WINDOW_MIN_BLOCKS)
+beam_window_kernel(const LaunchArgs a) {
+  using St = Staged<P, KS, MT, WS, NSTAGE, MAXRED, CHECKED, STORAGE>;
+  extern __shared__ __align__(128) unsigned char smem[];
+  const typename St::Smem sm = St::carve(smem, a.rowcap, a.max_active);
+  if (threadIdx.x == 0) St::init_barriers(sm);
+  __syncthreads();
+  const int tile = blockIdx.x % a.tab0.n_tiles;
+  const int chunk = blockIdx.x / a.tab0.n_tiles;
+  const int tau_first = a.rec0.out0 / St::TT;
+  const int tau_end = (a.rec0.out1 + St::TT - 1) / St::TT;
+  const int tau0 = tau_first + chunk * a.tiles_per_chunk;
+  const int tau1 = min(tau0 + a.tiles_per_chunk, tau_end);
+  St::run_item(sm, a.tab0, a.rec0, tile, tau0, tau1, a.rowcap, a.status, 0);
+}
+
+// Persistent launch: a fixed grid whose blocks pop work items from a device
+// queue until it is empty.  The queue is a counter over the items of all
+// records (record r owns items rec_prefix[r] .. rec_prefix[r + 1] - 1, each a
+// source tile x a chunk of r.tpc time tiles, time-chunk major).  Records may
+// differ in length, station subset and table; storage, phases and reduce are
+// the launch's.
+template <int P, int KS, int MT, int WS, int NSTAGE, bool MAXRED, bool CHECKED, int STORAGE>
+__global__ void __launch_bounds__((WS + 1) * 32, BP_WINDOW_MIN_BLOCKS)
+beam_batch_kernel(const LaunchArgs a) {
+  using St = Staged<P, KS, MT, WS, NSTAGE, MAXRED, CHECKED, STORAGE>;
+  extern __shared__ __align__(128) unsigned char smem[];
+  const typename St::Smem sm = St::carve(smem, a.rowcap, a.max_active);
+  if (threadIdx.x == 0) St::init_barriers(sm);
+  __syncthreads();
+  int it = 0;
+  const long long n_items = a.rec_prefix[a.n_records];
+  while (true) {
+    if (threadIdx.x == 0) {
+      const long long i = (long long)atomicAdd(a.next_item, 1ull);
+      int4 cur = make_int4(-1, 0, 0, 0);
+      if (i < n_items) {
+        // record r: rec_prefix[r] <= i < rec_prefix[r + 1]
+        int lo = 0, hi = a.n_records - 1;
+        while (lo < hi) {
+          const int mid = (lo + hi + 1) >> 1;
+          if (a.rec_prefix[mid] <= i) lo = mid; else hi = mid - 1;
+        }
+        const RecordView& r = a.records[lo];
+        const int n_tiles = a.tables[r.table].n_tiles;
+        const long long local = i - a.rec_prefix[lo];
+        const int chunk = (int)(local / n_tiles);
+        const int tile = (int)(local - (long long)chunk * n_tiles);
+        const int tau_first = r.out0 / St::TT;
+        const int tau_end = (r.out1 + St::TT - 1) / St::TT;
+        const int tau0 = tau_first + chunk * r.tpc;
+        cur = make_int4(lo, tile, tau0, min(tau0 + r.tpc, tau_end));
+      }
+      *sm.cur_item = cur;
+    }
+    __syncthreads();
+    const int4 item = *sm.cur_item;
+    if (item.x < 0) break;
+    const RecordView rc = a.records[item.x];
+    const TableView tb = a.tables[rc.table];
+    it += St::run_item(sm, tb, rc, item.y, item.z, item.w, a.rowcap, a.status, it);
+    __syncthreads();
+    if (*sm.abort_flag) break;
+  }
+}
+
+
+// Decode every record's keys of a batch into its outputs.
+__global__ void batch_decode_kernel(const RecordView* __restrict__ recs) {
+  const RecordView& r = recs[blockIdx.y];
+  const int n = r.out1 - r.out0;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    const unsigned long long k = r.keys[t];
+    if (k != 0ull) {
+      r.beam_max[t] = key_value(k);
+      r.argmax[t] = key_source(k);
+    } else {
+      r.argmax[t] = 0;
+    }
+  }
+}
+
+// Per tile slot (min, max) delay over the stations a record uses (weighted
+// and in its station mask), from the table itself: d = lo + offset.
+template <int P>
+__global__ void masked_minmax_kernel(TableView tb, int K, const uint32_t* __restrict__ mask,
+                                     int2* __restrict__ out) {
+  using M = typename MetaT<P>::type;
+  const long long slot = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (slot >= (long long)tb.n_tiles * K) return;
+  const int tile = (int)(slot / K), k = (int)(slot - (long long)tile * K);
+  const int n_act = tb.tile_hdr[tile].x;
+  const M* meta = reinterpret_cast<const M*>(tb.meta) + (size_t)tile * tb.S * K;
+  int mn = INT_MAX, mx = INT_MIN;
+  for (int j = 0; j < n_act; ++j) {
+    const int s = tb.st_s[(size_t)tile * tb.S + j];
+    if (mask && !((mask[s >> 5] >> (s & 31)) & 1u)) continue;
+    const M m = meta[(size_t)j * K + k];
+    if (__uint_as_float(m.x) == 0.0f) continue;
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+      const int d = tb.st_lo[((size_t)tile * tb.S + j) * P + p] + meta_off<P>(m, p);
+      mn = min(mn, d);
+      mx = max(mx, d);
+    }
+  }
+  out[slot] = make_int2(mn, mx);
 }
 
 // ---------------------------------------------------------------------------

@@ -181,6 +181,47 @@ BP_API int bp_beamform_dev(const bp_table *table, const void *d_traces, int stor
                     size_t pitch, int out_of_bounds, float *d_beam, size_t ldb,
                     void *stream);
 
+/* ---- batches of records (waveform windows, streamed chunks) ------------- */
+
+/* One record of a batch: a waveform window, or a streamed chunk together
+ * with the samples it carries over from the previous chunk.  Record sample t
+ * is global sample t_origin + t; the traces hold record samples
+ * [0, n_samples) in the layout of bp_trace_layout(table, n_samples); results
+ * are produced for record samples [out0, out1).  The strict rule's lower
+ * bound is applied in global time (t_origin + t + min >= 0), its upper bound
+ * in record time (t + max < n_samples).  A station mask restricts the record
+ * to a subset of the table's stations (as if weights_sources were zero for
+ * the others), without rebuilding the table.  No reference counterpart: the
+ * reference beamforms one window per call (beampower/beampower.py:10). */
+typedef struct bp_record {
+  int32_t table;                 /* index into the batch's tables             */
+  int32_t out_of_bounds;         /* 0 strict, 1 flexible                      */
+  const void *traces;            /* device                                    */
+  const float *scales;           /* device (S,), 16-bit storage only          */
+  size_t n_samples, lpad, pitch;
+  int64_t t_origin;
+  size_t out0, out1;
+  const uint32_t *station_mask;  /* device, ceil(S / 32) words, or NULL (all) */
+  float *beam_max;               /* device [out1 - out0]                      */
+  int32_t *argmax;               /* device [out1 - out0]                      */
+} bp_record;
+
+typedef struct bp_batch bp_batch;
+
+/* Upload the batch's descriptors and per-record delay ranges (stream-ordered
+ * device allocations; synchronises `stream` once). */
+BP_API int bp_batch_create(const bp_table *const *tables, int n_tables,
+                           const bp_record *records, int n_records, int storage,
+                           void *stream, bp_batch **out_batch);
+/* Beamform every record (reduce='max') in one persistent launch fed by a
+ * device work queue, then decode all outputs.  Only memsets and kernel
+ * launches on `stream`: it can be captured in a CUDA graph and replayed on
+ * new trace data in the same buffers. */
+BP_API int bp_batch_run(bp_batch *batch, void *stream);
+/* Kernel status bits of the batch's last runs (synchronises `stream`). */
+BP_API int bp_batch_status(bp_batch *batch, void *stream, int *status);
+BP_API int bp_batch_destroy(bp_batch *batch);
+
 /* Per-source (min, max) delay over weighted stations, (N, 2) int32, the
  * reference's _find_minmax_time_delays (beampower/src/beamform.c:10-47,
  * beamform.cu:28-65). */
