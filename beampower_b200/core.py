@@ -96,6 +96,7 @@ SIGNATURES = {
     "bp_batch_create": ([ct.POINTER(_vp), _int, ct.POINTER(Record), _int, _int, _vp,
                          ct.POINTER(_vp)], _int),
     "bp_batch_run": ([_vp, _vp], _int),
+    "bp_record_beamform_max_dev": ([_vp, ct.POINTER(Record), _int, _vp, _vp], _int),
     "bp_batch_status": ([_vp, _vp, ct.POINTER(_int)], _int),
     "bp_batch_destroy": ([_vp], _int),
     "bp_last_error": ([], ct.c_char_p),

@@ -1283,3 +1283,55 @@ int bp_batch_destroy(bp_batch* b) {
 }
 
 }  // extern "C"
+
+extern "C" {
+
+int bp_record_beamform_max_dev(const bp_table* t, const bp_record* q, int storage,
+                               unsigned long long* keys, void* stream) {
+  g_last_error.clear();
+  if (!t || !q || !keys) return fail(BP_ERR_INVALID_ARGUMENT, "NULL argument");
+  if (!t->info.uses_window_kernel)
+    return fail(BP_ERR_UNSUPPORTED, "records need a table that uses the staged kernel");
+  if (q->station_mask) return fail(BP_ERR_INVALID_ARGUMENT, "station masks need a batch");
+  if (q->out_of_bounds != 0 && q->out_of_bounds != 1)
+    return fail(BP_ERR_INVALID_ARGUMENT, "out_of_bounds must be 0 or 1");
+  if (q->out0 > q->out1 || q->out1 > q->n_samples || q->n_samples > (size_t)kMaxInt / 2)
+    return fail(BP_ERR_INVALID_ARGUMENT, "output range outside the record");
+  if (!q->traces || !q->beam_max || !q->argmax || (storage != BP_STORAGE_F32 && !q->scales))
+    return fail(BP_ERR_INVALID_ARGUMENT, "NULL pointer");
+  if (int rc = check_layout(t, q->n_samples, q->lpad, q->pitch)) return rc;
+  const size_t n_out = q->out1 - q->out0;
+  if (n_out == 0) return BP_OK;
+  cudaStream_t st = as_stream(stream);
+  BP_CUDA(cudaMemsetAsync(keys, 0, n_out * sizeof(unsigned long long), st));
+  bp::LaunchArgs a{};
+  a.tab0 = table_view(t);
+  bp::RecordView& r = a.rec0;
+  r.traces = q->traces;
+  r.scales = q->scales;
+  r.pitch = (long long)q->pitch;
+  r.t_origin = q->t_origin;
+  r.lpad = (int)q->lpad;
+  r.T = (int)q->n_samples;
+  r.out0 = (int)q->out0;
+  r.out1 = (int)q->out1;
+  r.flexible = q->out_of_bounds;
+  r.keys = keys;
+  const int tau_first = r.out0 / kTimeTile;
+  const int n_tt = (r.out1 + kTimeTile - 1) / kTimeTile - tau_first;
+  a.tiles_per_chunk = choose_tiles_per_chunk(n_tt, t->dev.n_tiles, t->device);
+  a.rowcap = rowcap_for(t);
+  a.max_active = std::max(1, t->info.max_active);
+  a.status = t->status;
+  const long long blocks =
+      (long long)((n_tt + a.tiles_per_chunk - 1) / a.tiles_per_chunk) * t->dev.n_tiles;
+  const bool checked = q->out_of_bounds && t->info.any_nonfinite;
+  if (int rc = launch_window<true>(t->dev.P, checked, storage, a, false, blocks, t->device, st))
+    return rc;
+  bp::decode_keys_kernel<<<(unsigned)((n_out + 255) / 256), 256, 0, st>>>(
+      keys, (int)n_out, q->beam_max, q->argmax);
+  BP_LAUNCHED("decode_keys_kernel");
+  return BP_OK;
+}
+
+}  // extern "C"

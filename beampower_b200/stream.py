@@ -1,0 +1,243 @@
+"""Stream scheduler: waveform chunks from several networks, beamformed as they
+arrive, with results identical to one offline call on the whole record.
+
+Per network (``NetworkStream``) the travel-time table and weights stay
+resident in HBM and the last samples of raw features are carried from chunk
+to chunk.  Output sample g needs trace samples up to g + max_delay, so after
+a chunk has brought the record to t_end samples the stream emits the samples
+g < t_end - max_delay: for those every (source, station, phase) term the
+offline call would use is available, so the emitted beams are the offline
+beams, bit for bit with FP32 storage (strict and flexible rules alike).  The
+carried part is the features from (next g to emit) + min(0, min_delay) on.
+``flush()`` ends the record and emits the rest with the record's true length.
+
+``StreamScheduler`` is the request loop over many networks (continuous
+batching): chunks are queued on arrival and admitted while fewer than
+``max_inflight`` chunks are on the GPU and their memory fits the budget; each
+network's chunks run in order on its own CUDA stream, chunks of different
+networks overlap on the device.  Latency is arrival (host clock) to the
+completion event of the chunk's last kernel (device clock, mapped to the host
+clock once).
+"""
+from __future__ import annotations
+
+import collections
+import ctypes as ct
+import time
+
+import numpy as np
+
+from .core import STORAGE, Record, check, load_library
+from .tables import TravelTimeTable, _dev_tensor, _stream_ptr
+
+try:
+    import torch
+except ImportError:  # pragma: no cover
+    torch = None
+
+
+class NetworkStream:
+    """Streaming state of one network.
+
+    Parameters
+    ----------
+    table: TravelTimeTable of the network (resident delays and weights)
+    weights_phases: (S, C, P) channel -> phase weights
+    out_of_bounds: 'strict' or 'flexible'
+    storage: 'fp32', 'bf16' or 'fp16'
+    """
+
+    def __init__(self, table: TravelTimeTable, weights_phases, out_of_bounds="strict",
+                 storage="fp32", name=None):
+        if torch is None:
+            raise RuntimeError("torch is required for streaming")
+        self.lib = load_library("gpu")
+        self.table = table
+        self.name = name
+        self.device = table.device
+        self.alpha = _dev_tensor(weights_phases, torch.float32, self.device)
+        self.S, self.C, self.P = map(int, self.alpha.shape)
+        self.oob = 0 if out_of_bounds == "strict" else 1
+        self.storage = storage
+        self._st = STORAGE[storage]
+        info = table.info
+        weighted = info["min_delay"] <= info["max_delay"]
+        self.lead = min(0, info["min_delay"]) if weighted else 0   # <= 0
+        self.lag = max(0, info["max_delay"]) if weighted else 0    # >= 0
+        self.t_end = 0     # samples received
+        self.t_emit = 0    # next sample to emit
+        self.carry = torch.zeros((self.S, self.C, -self.lead), dtype=torch.float32,
+                                 device=self.device)  # global [t_emit + lead, t_end)
+        self.stream = torch.cuda.Stream(device=self.device)
+        self.results = []  # (g0, beam_max, argmax) device tensors, in order
+
+    def bytes_per_chunk(self, n_samples):
+        """Device bytes one chunk holds while in flight (record + traces + outputs)."""
+        rec = n_samples + self.lag - self.lead
+        elem = 4 if self._st == 0 else 4  # 16-bit storage keeps two versions
+        return (self.S * self.C * rec * 4 + self.S * self.P * (rec + 1024 + self.lag) * elem
+                + n_samples * 16)
+
+    def _beamform(self, record, base, out_lo, out_hi):
+        """Beamform record samples [out_lo, out_hi) of a record starting at
+        global sample `base`.  Enqueued on the current stream."""
+        T = int(record.shape[2])
+        lpad, pitch = self.table.layout(T)
+        st = self._st
+        rows = self.S * self.P * (1 if st == 0 else 2)
+        elem = torch.float32 if st == 0 else (torch.bfloat16 if st == 1 else torch.float16)
+        traces = torch.empty((rows, pitch), dtype=elem, device=self.device)
+        scales = torch.ones(self.S, dtype=torch.float32, device=self.device)
+        sp = _stream_ptr()
+        check(self.lib.bp_prestack_dev(record.data_ptr(), self.alpha.data_ptr(), T, self.S,
+                                       self.C, self.P, st, lpad, pitch, traces.data_ptr(),
+                                       scales.data_ptr(), sp))
+        n = out_hi - out_lo
+        bm = torch.zeros(n, dtype=torch.float32, device=self.device)
+        am = torch.zeros(n, dtype=torch.int32, device=self.device)
+        keys = torch.empty(max(n, 1), dtype=torch.int64, device=self.device)
+        r = Record()
+        r.table = 0
+        r.out_of_bounds = self.oob
+        r.traces = traces.data_ptr()
+        r.scales = scales.data_ptr()
+        r.n_samples = T
+        r.lpad = lpad
+        r.pitch = pitch
+        r.t_origin = base
+        r.out0 = out_lo
+        r.out1 = out_hi
+        r.station_mask = None
+        r.beam_max = bm.data_ptr()
+        r.argmax = am.data_ptr()
+        check(self.lib.bp_record_beamform_max_dev(self.table.handle, ct.byref(r), st,
+                                                  keys.data_ptr(), sp))
+        # keep the temporaries alive until the stream has used them
+        for t in (traces, scales, keys, record):
+            t.record_stream(torch.cuda.current_stream())
+        return bm, am
+
+    def push(self, chunk):
+        """Append an (S, C, L) chunk (numpy, host or device tensor); enqueue the
+        work on this network's stream.  Returns the emitted (g0, beam_max,
+        argmax) or None."""
+        with torch.cuda.stream(self.stream):
+            if isinstance(chunk, np.ndarray):
+                chunk = torch.from_numpy(np.ascontiguousarray(chunk, dtype=np.float32))
+            chunk = chunk.to(self.device, dtype=torch.float32, non_blocking=True)
+            L = int(chunk.shape[2])
+            base = self.t_emit + self.lead
+            record = torch.cat([self.carry, chunk], dim=2)  # global [base, t_end + L)
+            self.t_end += L
+            emit_to = self.t_end - self.lag
+            out = None
+            if emit_to > self.t_emit:
+                bm, am = self._beamform(record, base, self.t_emit - base, emit_to - base)
+                out = (self.t_emit, bm, am)
+                self.results.append(out)
+                self.t_emit = emit_to
+            new_base = self.t_emit + self.lead
+            self.carry = record[:, :, new_base - base:].contiguous()
+        return out
+
+    def flush(self):
+        """End of the record: emit every remaining sample."""
+        with torch.cuda.stream(self.stream):
+            base = self.t_emit + self.lead
+            out = None
+            if self.t_end > self.t_emit:
+                bm, am = self._beamform(self.carry.contiguous(), base, self.t_emit - base,
+                                        self.t_end - base)
+                out = (self.t_emit, bm, am)
+                self.results.append(out)
+                self.t_emit = self.t_end
+        return out
+
+    def collect(self):
+        """All emitted results as numpy arrays (synchronises the stream)."""
+        self.stream.synchronize()
+        if not self.results:
+            return np.zeros(0, np.float32), np.zeros(0, np.int32)
+        bm = torch.cat([r[1] for r in self.results]).cpu().numpy()
+        am = torch.cat([r[2] for r in self.results]).cpu().numpy()
+        return bm, am
+
+
+class StreamScheduler:
+    """Continuous batching of chunks from many networks.
+
+    networks: dict name -> NetworkStream
+    max_inflight: chunks admitted to the GPU at once
+    memory_budget: device bytes the in-flight chunks may hold
+    """
+
+    def __init__(self, networks, max_inflight=8, memory_budget=150e9):
+        self.networks = dict(networks)
+        self.max_inflight = max_inflight
+        self.memory_budget = memory_budget
+        self.pending = collections.deque()  # (arrival, name, chunk)
+        self.inflight = []  # (arrival, name, event, bytes, terms)
+        self.mem_in_use = 0
+        self.done = []  # (name, arrival, completion, terms)
+        dev = next(iter(self.networks.values())).device
+        self.device = dev
+        # device clock -> host clock
+        torch.cuda.synchronize(dev)
+        self._ev0 = torch.cuda.Event(enable_timing=True)
+        self._ev0.record(torch.cuda.current_stream(dev))
+        torch.cuda.synchronize(dev)
+        self._host0 = time.perf_counter()
+
+    def submit(self, name, chunk, arrival=None):
+        self.pending.append((time.perf_counter() if arrival is None else arrival, name, chunk))
+
+    def _admit(self):
+        while self.pending and len(self.inflight) < self.max_inflight:
+            arrival, name, chunk = self.pending[0]
+            net = self.networks[name]
+            need = net.bytes_per_chunk(int(chunk.shape[2]))
+            free, _ = torch.cuda.mem_get_info(self.device)
+            if self.inflight and (self.mem_in_use + need > self.memory_budget or need > free):
+                break  # wait for memory to free up
+            self.pending.popleft()
+            t_emit0 = net.t_emit
+            net.push(chunk)
+            terms = (net.t_emit - t_emit0) * net.table.n_sources * net.S * net.P
+            ev = torch.cuda.Event(enable_timing=True)
+            ev.record(net.stream)
+            self.inflight.append((arrival, name, ev, need, terms))
+            self.mem_in_use += need
+
+    def _retire(self):
+        keep = []
+        for item in self.inflight:
+            arrival, name, ev, need, terms = item
+            if ev.query():
+                done_t = self._host0 + self._ev0.elapsed_time(ev) / 1e3
+                self.done.append((name, arrival, done_t, terms))
+                self.mem_in_use -= need
+            else:
+                keep.append(item)
+        self.inflight = keep
+
+    def step(self):
+        self._retire()
+        self._admit()
+
+    def drain(self):
+        while self.pending or self.inflight:
+            self.step()
+            if self.inflight:
+                time.sleep(1e-4)
+
+    def stats(self):
+        if not self.done:
+            return {}
+        lat = np.array([c - a for _, a, c, _ in self.done])
+        t0 = min(a for _, a, _, _ in self.done)
+        t1 = max(c for _, _, c, _ in self.done)
+        terms = sum(t for *_, t in self.done)
+        return {"chunks": len(self.done), "p50_ms": float(np.percentile(lat, 50) * 1e3),
+                "p99_ms": float(np.percentile(lat, 99) * 1e3),
+                "max_ms": float(lat.max() * 1e3), "terms": terms,
+                "terms_per_s": terms / max(t1 - t0, 1e-9), "span_s": t1 - t0}

@@ -208,6 +208,15 @@ typedef struct bp_record {
 
 typedef struct bp_batch bp_batch;
 
+/* One record alone (no batch): the plain staged launch over the record's
+ * output range, global time origin included; this is what a streamed chunk
+ * with its carried samples uses.  d_keys: (out1 - out0) uint64 scratch,
+ * cleared here.  station_mask must be NULL.  Stream-ordered, no allocation,
+ * no synchronisation. */
+BP_API int bp_record_beamform_max_dev(const bp_table *table, const bp_record *record,
+                                      int storage, unsigned long long *d_keys,
+                                      void *stream);
+
 /* Upload the batch's descriptors and per-record delay ranges (stream-ordered
  * device allocations; synchronises `stream` once). */
 BP_API int bp_batch_create(const bp_table *const *tables, int n_tables,
