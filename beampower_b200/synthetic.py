@@ -183,3 +183,186 @@ def digest(*arrays: np.ndarray) -> str:
 def nominal_terms(n_sources: int, n_samples: int, n_stations: int, n_phases: int) -> int:
     """Beam terms of one call: sources x samples x stations x phases."""
     return int(n_sources) * int(n_samples) * int(n_stations) * int(n_phases)
+
+
+# ---------------------------------------------------------------------------
+# Batching workload: many detection windows over one 100-station network and
+# two source grids (400,000 and 50,000 points).  Each window has a seeded
+# length of 1-30 min at 50 Hz, a station subset of 20-80 stations (applied
+# as zero weights / a station mask) and 1-5 injected events.
+# ---------------------------------------------------------------------------
+@dataclass(frozen=True)
+class BatchSpec:
+    name: str = "batch-128-windows-100-sta-400k-and-50k-src"
+    n_stations: int = 100
+    square_km: float = 150.0
+    fs: float = 50.0
+    grids: tuple = ((100, 100, 40, 40.0), (50, 50, 20, 20.0))  # (nx, ny, nz, depth_km)
+    n_windows: int = 128
+    t_range: tuple = (3000, 90000)
+    subset: tuple = (20, 80)
+    events: tuple = (1, 5)
+    seed: int = 0
+
+
+BATCH = BatchSpec()
+
+
+def make_batch_workload(spec: BatchSpec = BATCH, n_windows: int | None = None):
+    """Stations, per-grid (delays, weights) and the window list.
+
+    Windows are dicts {table, n_samples, stations (sorted list), events
+    [(source, origin)], seed}; their features are drawn by
+    ``window_features`` (numpy) or ``window_features_torch`` (device)."""
+    rng = np.random.default_rng(spec.seed)
+    S = spec.n_stations
+    stations = np.zeros((S, 3))
+    stations[:, :2] = rng.uniform(0.0, spec.square_km, size=(S, 2))
+    grids = []
+    for nx, ny, nz, depth in spec.grids:
+        g = NetworkSpec("grid", S, spec.square_km, spec.fs, 1, (nx, ny, nz), depth, 0)
+        src = source_grid(g)
+        D = travel_time_delays(stations, src, spec.fs)
+        W = np.ones((src.shape[0], S), dtype=np.float32)
+        grids.append((D, W))
+    alpha = np.zeros((S, 3, 2), dtype=np.float32)
+    alpha[:, 0, 0] = 1.0
+    alpha[:, 1:, 1] = 1.0
+    windows = []
+    n = spec.n_windows if n_windows is None else n_windows
+    for i in range(n):
+        table = int(rng.integers(0, len(grids)))
+        T = int(rng.integers(spec.t_range[0], spec.t_range[1] + 1))
+        k = int(rng.integers(spec.subset[0], spec.subset[1] + 1))
+        st = sorted(int(s) for s in rng.choice(S, size=k, replace=False))
+        D = grids[table][0]
+        evs = []
+        for _ in range(int(rng.integers(spec.events[0], spec.events[1] + 1))):
+            src = int(rng.integers(0, D.shape[0]))
+            dmax = int(D[src].max())
+            if T - dmax - 40 > 40:
+                evs.append((src, int(rng.integers(40, T - dmax - 40))))
+        windows.append({"table": table, "n_samples": T, "stations": st, "events": evs,
+                        "seed": int(rng.integers(0, 2**31 - 1))})
+    return {"stations": stations, "grids": grids, "weights_phases": alpha,
+            "windows": windows, "spec": spec}
+
+
+def window_features(wl, i):
+    """(S, 3, T) float32 features of window i (numpy)."""
+    w = wl["windows"][i]
+    S = wl["spec"].n_stations
+    rng = np.random.default_rng(w["seed"])
+    F = _smooth(np.abs(rng.standard_normal((S, 3, w["n_samples"]), dtype=np.float32)), SMOOTH)
+    _inject(F, wl["grids"][w["table"]][0], w["events"])
+    return F
+
+
+def window_features_torch(wl, i, device):
+    """(S, 3, T) float32 features of window i drawn on the device (seeded,
+    not bit-identical to ``window_features``)."""
+    import torch
+    w = wl["windows"][i]
+    S = wl["spec"].n_stations
+    g = torch.Generator(device=device)
+    g.manual_seed(w["seed"])
+    x = torch.randn((S * 3, 1, w["n_samples"]), generator=g, device=device).abs_()
+    k = torch.full((1, 1, SMOOTH), 1.0 / SMOOTH, device=device)
+    F = torch.nn.functional.conv1d(x, k, padding=SMOOTH // 2)[:, 0, :w["n_samples"]]
+    F = F.reshape(S, 3, w["n_samples"]).contiguous()
+    D = wl["grids"][w["table"]][0]
+    half = int(np.ceil(6 * PULSE_SIGMA))
+    taps = torch.arange(-half, half + 1, device=device, dtype=torch.float32)
+    pulse = PULSE_AMPLITUDE * torch.exp(-0.5 * (taps / PULSE_SIGMA) ** 2)
+    for src, t0 in w["events"]:
+        for s in range(S):
+            for ch, ph in ((0, 0), (1, 1), (2, 1)):
+                c = t0 + int(D[src, s, ph])
+                lo, hi = c - half, c + half + 1
+                a, b = max(lo, 0), min(hi, w["n_samples"])
+                if a < b:
+                    F[s, ch, a:b] += pulse[a - lo:b - lo]
+    return F
+
+
+def _inject(F, D, events):
+    S, _, T = F.shape
+    half = int(np.ceil(6 * PULSE_SIGMA))
+    taps = np.arange(-half, half + 1)
+    pulse = (PULSE_AMPLITUDE * np.exp(-0.5 * (taps / PULSE_SIGMA) ** 2)).astype(np.float32)
+    for src, t0 in events:
+        for s in range(S):
+            for ch, ph in ((0, 0), (1, 1), (2, 1)):
+                c = t0 + int(D[src, s, ph])
+                lo, hi = c - half, c + half + 1
+                a, b = max(lo, 0), min(hi, T)
+                if a < b:
+                    F[s, ch, a:b] += pulse[a - lo:b - lo]
+
+
+# ---------------------------------------------------------------------------
+# Serving workload: 8 networks of 30-100 stations, grids of 50,000-400,000
+# sources, sampling rates of 20, 50 or 100 Hz, 60 s chunks arriving as
+# Poisson processes that total ~200 chunks/s, events at 0.1 per minute.
+# ---------------------------------------------------------------------------
+@dataclass(frozen=True)
+class ServingSpec:
+    name: str = "serving-8-networks-60s-chunks"
+    n_networks: int = 8
+    stations: tuple = (30, 100)
+    grids: tuple = ((50, 50, 20), (100, 50, 20), (100, 100, 20), (100, 100, 40))
+    fs: tuple = (20.0, 50.0, 100.0)
+    chunk_s: float = 60.0
+    total_rate: float = 200.0  # chunks / s over all networks
+    events_per_min: float = 0.1
+    square_km: float = 150.0
+    depth_km: float = 40.0
+    seed: int = 0
+
+
+SERVING = ServingSpec()
+
+
+def make_serving_networks(spec: ServingSpec = SERVING):
+    """Per network: name, stations, fs, chunk length, delays (N, S, 2),
+    weights (N, S), weights_phases and its Poisson rate (chunks / s)."""
+    rng = np.random.default_rng(spec.seed)
+    rates = rng.uniform(0.5, 1.5, size=spec.n_networks)
+    rates *= spec.total_rate / rates.sum()
+    nets = []
+    for i in range(spec.n_networks):
+        S = int(rng.integers(spec.stations[0], spec.stations[1] + 1))
+        fs = float(spec.fs[int(rng.integers(0, len(spec.fs)))])
+        nx, ny, nz = spec.grids[int(rng.integers(0, len(spec.grids)))]
+        st = np.zeros((S, 3))
+        st[:, :2] = rng.uniform(0.0, spec.square_km, size=(S, 2))
+        g = NetworkSpec("grid", S, spec.square_km, fs, 1, (nx, ny, nz), spec.depth_km, 0)
+        D = travel_time_delays(st, source_grid(g), fs)
+        W = np.ones((D.shape[0], S), dtype=np.float32)
+        A = np.zeros((S, 3, 2), dtype=np.float32)
+        A[:, 0, 0] = 1.0
+        A[:, 1:, 1] = 1.0
+        nets.append({"name": f"net{i}", "n_stations": S, "fs": fs,
+                     "chunk": int(round(spec.chunk_s * fs)), "delays": D, "weights": W,
+                     "weights_phases": A, "rate": float(rates[i]),
+                     "seed": int(rng.integers(0, 2**31 - 1))})
+    return nets
+
+
+def serving_record(net, n_chunks, events_per_min=SERVING.events_per_min):
+    """A continuous (S, 3, n_chunks * chunk) record for one network with
+    Poisson events, to be cut into chunks."""
+    rng = np.random.default_rng(net["seed"])
+    S, L = net["n_stations"], net["chunk"]
+    T = n_chunks * L
+    F = _smooth(np.abs(rng.standard_normal((S, 3, T), dtype=np.float32)), SMOOTH)
+    n_ev = rng.poisson(events_per_min * T / net["fs"] / 60.0)
+    D = net["delays"]
+    evs = []
+    for _ in range(int(n_ev)):
+        src = int(rng.integers(0, D.shape[0]))
+        dmax = int(D[src].max())
+        if T - dmax - 40 > 40:
+            evs.append((src, int(rng.integers(40, T - dmax - 40))))
+    _inject(F, D, evs)
+    return F, evs
