@@ -99,6 +99,11 @@ SIGNATURES = {
     "bp_record_beamform_max_dev": ([_vp, ct.POINTER(Record), _int, _vp, _vp], _int),
     "bp_batch_status": ([_vp, _vp, ct.POINTER(_int)], _int),
     "bp_batch_destroy": ([_vp], _int),
+    "bp_kernel_config_count": ([], _int),
+    "bp_kernel_config_describe": ([_int, ct.POINTER(_int), ct.POINTER(_int), ct.POINTER(_int),
+                                   ct.POINTER(_int)], _int),
+    "bp_set_kernel_config": ([_int, _int, _int], _int),
+    "bp_get_kernel_config": ([_int, _int], _int),
     "bp_last_error": ([], ct.c_char_p),
     "bp_version": ([], ct.c_char_p),
     "bp_launch_count": ([], ct.c_uint64),

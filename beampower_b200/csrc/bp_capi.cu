@@ -55,16 +55,45 @@ inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s
 
 constexpr long long kMaxInt = std::numeric_limits<int>::max();
 
-// ---- default staged-kernel configuration -----------------------------------
-// 8 consumer warps x 8 sources per thread = 64 sources per tile, 8 samples
-// per lane = 256-sample time tiles, 4-stage ring.
+// ---- staged-kernel configurations --------------------------------------------
+// All use 64-source tiles (the table's tile size).  Config 0: 8 consumer warps
+// x 8 sources per thread, 8 samples per lane (256-sample time tiles), 2 blocks
+// per SM.  Config 1: 16 consumer warps x 4 sources, 16 samples per lane
+// (512-sample time tiles), 1 block per SM: twice the terms per metadata load.
 #ifndef BP_NSTAGE
 #define BP_NSTAGE 4
 #endif
-constexpr int kKS = 8, kMT = 8, kWS = 8, kNStage = BP_NSTAGE;
-constexpr int kTileSources = kWS * kKS;
-constexpr int kTimeTile = 32 * kMT;
-static_assert(bp::kMaxTimeTile % kTimeTile == 0, "time tile must divide kMaxTimeTile");
+template <int ID> struct KCfg;
+template <> struct KCfg<0> {
+  static constexpr int KS = 8, MT = 8, WS = 8, NSTAGE = BP_NSTAGE, MINB = 2;
+};
+template <> struct KCfg<1> {
+  static constexpr int KS = 4, MT = 16, WS = 16, NSTAGE = BP_NSTAGE, MINB = 1;
+};
+constexpr int kNumConfigs = 2;
+constexpr int kTileSources = 64;
+static_assert(KCfg<0>::KS * KCfg<0>::WS == kTileSources, "tile size");
+static_assert(KCfg<1>::KS * KCfg<1>::WS == kTileSources, "tile size");
+
+inline int cfg_time_tile(int cfg) { return cfg == 1 ? 32 * KCfg<1>::MT : 32 * KCfg<0>::MT; }
+
+// Preferred config per (storage, reduce); -1 = built-in default.
+std::atomic<int> g_cfg_choice[3][2] = {{{-1}, {-1}}, {{-1}, {-1}}, {{-1}, {-1}}};
+
+int pick_config(int storage, bool maxred) {
+  if (const char* v = std::getenv("BEAMPOWER_B200_KERNEL_CONFIG")) {
+    const int c = std::atoi(v);
+    if (c >= 0 && c < kNumConfigs) return c;
+  }
+  if (storage >= 0 && storage < 3) {
+    const int c = g_cfg_choice[storage][maxred ? 1 : 0].load();
+    if (c >= 0 && c < kNumConfigs) return c;
+  }
+  // Built-in defaults, measured on B200 (400,000 sources x 60 stations):
+  // FP32 storage is shared-memory bound and favours config 0; 16-bit storage
+  // is issue bound and gains from config 1's longer time tiles.
+  return storage == BP_STORAGE_F32 ? 0 : 1;
+}
 
 int device_sm_count(int dev) {
   static int cache[64] = {0};
@@ -251,16 +280,18 @@ int build_tiling_map(const int32_t* d_delays, const float* d_w, size_t N, size_t
 }
 
 // ---- staged kernel dispatch -------------------------------------------------
-template <int P, bool MAXRED, bool CHECKED, int STORAGE>
+template <int CFG, int P, bool MAXRED, bool CHECKED, int STORAGE>
 int launch_window_p(const bp::LaunchArgs& a, bool batch, long long plain_blocks, int dev,
                     cudaStream_t st) {
-  using L = bp::WindowSmem<P, kKS, kMT, kWS, kNStage, MAXRED>;
+  using C = KCfg<CFG>;
+  using L = bp::WindowSmem<P, C::KS, C::MT, C::WS, C::NSTAGE, MAXRED>;
   const L lay(a.rowcap, a.max_active);
   if (lay.total > (size_t)device_smem_optin(dev))
     return fail(BP_ERR_UNSUPPORTED, "staged kernel needs %zu B of shared memory", lay.total);
-  constexpr int threads = bp::WindowCfg<P, kKS, kMT, kWS>::kThreads;
+  constexpr int threads = bp::WindowCfg<P, C::KS, C::MT, C::WS>::kThreads;
   if (batch) {
-    auto kern = bp::beam_batch_kernel<P, kKS, kMT, kWS, kNStage, MAXRED, CHECKED, STORAGE>;
+    auto kern = bp::beam_batch_kernel<P, C::KS, C::MT, C::WS, C::NSTAGE, C::MINB, MAXRED,
+                                      CHECKED, STORAGE>;
     BP_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)lay.total));
     int per_sm = 0;
@@ -269,7 +300,8 @@ int launch_window_p(const bp::LaunchArgs& a, bool batch, long long plain_blocks,
     kern<<<grid, threads, lay.total, st>>>(a);
     BP_LAUNCHED("beam_batch_kernel");
   } else {
-    auto kern = bp::beam_window_kernel<P, kKS, kMT, kWS, kNStage, MAXRED, CHECKED, STORAGE>;
+    auto kern = bp::beam_window_kernel<P, C::KS, C::MT, C::WS, C::NSTAGE, C::MINB, MAXRED,
+                                       CHECKED, STORAGE>;
     BP_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)lay.total));
     if (plain_blocks > kMaxInt) return fail(BP_ERR_UNSUPPORTED, "grid too large");
@@ -280,51 +312,79 @@ int launch_window_p(const bp::LaunchArgs& a, bool batch, long long plain_blocks,
   return BP_OK;
 }
 
-template <bool MAXRED, bool CHECKED, int STORAGE>
+template <int CFG, bool MAXRED, bool CHECKED, int STORAGE>
 int launch_window_s(int P, const bp::LaunchArgs& a, bool batch, long long blocks, int dev,
                     cudaStream_t st) {
   switch (P) {
-    case 1: return launch_window_p<1, MAXRED, CHECKED, STORAGE>(a, batch, blocks, dev, st);
-    case 2: return launch_window_p<2, MAXRED, CHECKED, STORAGE>(a, batch, blocks, dev, st);
-    case 3: return launch_window_p<3, MAXRED, CHECKED, STORAGE>(a, batch, blocks, dev, st);
-    case 4: return launch_window_p<4, MAXRED, CHECKED, STORAGE>(a, batch, blocks, dev, st);
+    case 1: return launch_window_p<CFG, 1, MAXRED, CHECKED, STORAGE>(a, batch, blocks, dev, st);
+    case 2: return launch_window_p<CFG, 2, MAXRED, CHECKED, STORAGE>(a, batch, blocks, dev, st);
+    case 3: return launch_window_p<CFG, 3, MAXRED, CHECKED, STORAGE>(a, batch, blocks, dev, st);
+    case 4: return launch_window_p<CFG, 4, MAXRED, CHECKED, STORAGE>(a, batch, blocks, dev, st);
     default: return fail(BP_ERR_UNSUPPORTED, "staged kernel supports 1..4 phases");
   }
 }
 
-template <bool MAXRED>
-int launch_window(int P, bool checked, int storage, const bp::LaunchArgs& a, bool batch,
-                  long long blocks, int dev, cudaStream_t st) {
+template <int CFG, bool MAXRED>
+int launch_window_c(int P, bool checked, int storage, const bp::LaunchArgs& a, bool batch,
+                    long long blocks, int dev, cudaStream_t st) {
   if (storage == BP_STORAGE_F32)
-    return checked ? launch_window_s<MAXRED, true, BP_STORAGE_F32>(P, a, batch, blocks, dev, st)
-                   : launch_window_s<MAXRED, false, BP_STORAGE_F32>(P, a, batch, blocks, dev, st);
+    return checked
+               ? launch_window_s<CFG, MAXRED, true, BP_STORAGE_F32>(P, a, batch, blocks, dev, st)
+               : launch_window_s<CFG, MAXRED, false, BP_STORAGE_F32>(P, a, batch, blocks, dev, st);
   if (checked)
     return fail(BP_ERR_UNSUPPORTED,
                 "non-finite weights in flexible mode need FP32 trace storage");
   if (storage == BP_STORAGE_BF16)
-    return launch_window_s<MAXRED, false, BP_STORAGE_BF16>(P, a, batch, blocks, dev, st);
+    return launch_window_s<CFG, MAXRED, false, BP_STORAGE_BF16>(P, a, batch, blocks, dev, st);
   if (storage == BP_STORAGE_F16)
-    return launch_window_s<MAXRED, false, BP_STORAGE_F16>(P, a, batch, blocks, dev, st);
+    return launch_window_s<CFG, MAXRED, false, BP_STORAGE_F16>(P, a, batch, blocks, dev, st);
   return fail(BP_ERR_INVALID_ARGUMENT, "unknown storage %d", storage);
 }
 
-int staged_smem_bytes(int P, bool maxred, int rowcap, int max_active) {
-  auto f = [&](auto tag) -> size_t {
-    constexpr int PP = decltype(tag)::value;
-    if (maxred) return bp::WindowSmem<PP, kKS, kMT, kWS, kNStage, true>(rowcap, max_active).total;
-    return bp::WindowSmem<PP, kKS, kMT, kWS, kNStage, false>(rowcap, max_active).total;
-  };
-  switch (P) {
-    case 1: return (int)f(std::integral_constant<int, 1>{});
-    case 2: return (int)f(std::integral_constant<int, 2>{});
-    case 3: return (int)f(std::integral_constant<int, 3>{});
-    case 4: return (int)f(std::integral_constant<int, 4>{});
-  }
-  return INT_MAX;
+template <bool MAXRED>
+int launch_window(int cfg, int P, bool checked, int storage, const bp::LaunchArgs& a,
+                  bool batch, long long blocks, int dev, cudaStream_t st) {
+  if (cfg == 1)
+    return launch_window_c<1, MAXRED>(P, checked, storage, a, batch, blocks, dev, st);
+  return launch_window_c<0, MAXRED>(P, checked, storage, a, batch, blocks, dev, st);
 }
 
-int rowcap_for(const bp_table* t) {
-  return (int)bp::align_up_sz((size_t)(kTimeTile + t->info.max_spread + 1), bp::kAlign);
+template <int CFG>
+size_t staged_smem_cfg(int P, bool maxred, int rowcap, int max_active) {
+  using C = KCfg<CFG>;
+  auto f = [&](auto tag) -> size_t {
+    constexpr int PP = decltype(tag)::value;
+    if (maxred)
+      return bp::WindowSmem<PP, C::KS, C::MT, C::WS, C::NSTAGE, true>(rowcap, max_active).total;
+    return bp::WindowSmem<PP, C::KS, C::MT, C::WS, C::NSTAGE, false>(rowcap, max_active).total;
+  };
+  switch (P) {
+    case 1: return f(std::integral_constant<int, 1>{});
+    case 2: return f(std::integral_constant<int, 2>{});
+    case 3: return f(std::integral_constant<int, 3>{});
+    case 4: return f(std::integral_constant<int, 4>{});
+  }
+  return SIZE_MAX;
+}
+
+size_t staged_smem_bytes(int cfg, int P, bool maxred, int rowcap, int max_active) {
+  return cfg == 1 ? staged_smem_cfg<1>(P, maxred, rowcap, max_active)
+                  : staged_smem_cfg<0>(P, maxred, rowcap, max_active);
+}
+
+int rowcap_for(const bp_table* t, int cfg) {
+  return (int)bp::align_up_sz((size_t)(cfg_time_tile(cfg) + t->info.max_spread + 1),
+                              bp::kAlign);
+}
+
+// The preferred config if its shared memory fits this table, else config 0.
+int config_for(const bp_table* t, int storage, bool maxred) {
+  const int c = pick_config(storage, maxred);
+  if (c != 0 && staged_smem_bytes(c, t->dev.P, maxred, rowcap_for(t, c),
+                                  std::max(1, t->info.max_active)) >
+                     (size_t)device_smem_optin(t->device))
+    return 0;
+  return c;
 }
 
 int choose_tiles_per_chunk(int n_tt, int n_tiles, int dev) {
@@ -380,17 +440,21 @@ int run_staged(const bp_table* t, const void* traces, int storage, const float* 
   r.keys = keys;
   r.beam = beam;
   r.ldb = (long long)ldb;
-  const int n_tt = (int)((T + kTimeTile - 1) / kTimeTile);
+  const bool maxred = keys != nullptr;
+  const int cfg = config_for(t, storage, maxred);
+  const int tt = cfg_time_tile(cfg);
+  const int n_tt = (int)((T + tt - 1) / tt);
   a.tiles_per_chunk = choose_tiles_per_chunk(n_tt, t->dev.n_tiles, t->device);
-  a.rowcap = rowcap_for(t);
+  a.rowcap = rowcap_for(t, cfg);
   a.max_active = std::max(1, t->info.max_active);
   a.status = t->status;
   if (n_tt == 0) return BP_OK;
   const long long blocks =
       (long long)((n_tt + a.tiles_per_chunk - 1) / a.tiles_per_chunk) * t->dev.n_tiles;
   const bool checked = out_of_bounds && t->info.any_nonfinite;
-  if (keys) return launch_window<true>(t->dev.P, checked, storage, a, false, blocks, t->device, st);
-  return launch_window<false>(t->dev.P, checked, storage, a, false, blocks, t->device, st);
+  if (maxred)
+    return launch_window<true>(cfg, t->dev.P, checked, storage, a, false, blocks, t->device, st);
+  return launch_window<false>(cfg, t->dev.P, checked, storage, a, false, blocks, t->device, st);
 }
 
 int run_direct(const void* traces, int storage, const float* scales, size_t T, size_t lpad,
@@ -622,9 +686,10 @@ int bp_table_create(const int32_t* d_delays, const float* d_weights, size_t N, s
   in.any_nonfinite = stats[bp::kStatNonFinite];
   bool use_window = window && n_tiles > 0 && !stats[bp::kStatWideTile];
   if (use_window) {
-    const int rowcap = (int)bp::align_up_sz((size_t)(kTimeTile + in.max_spread + 1), bp::kAlign);
-    const int need = staged_smem_bytes((int)P, true, rowcap, std::max(1, in.max_active));
-    if (need > device_smem_optin(t->device)) use_window = false;
+    const int rowcap = (int)bp::align_up_sz((size_t)(cfg_time_tile(0) + in.max_spread + 1),
+                                            bp::kAlign);
+    const size_t need = staged_smem_bytes(0, (int)P, true, rowcap, std::max(1, in.max_active));
+    if (need > (size_t)device_smem_optin(t->device)) use_window = false;
   }
   in.uses_window_kernel = use_window ? 1 : 0;
   if (!use_window && N > 0) {
@@ -1072,6 +1137,7 @@ struct bp_batch {
   int storage;
   int n_records;
   int rowcap;
+  int cfg;
   int max_active;
   bool checked;
   void* mem;                        // device: tables, records, prefix, keys, srcmm, queue, status
@@ -1086,7 +1152,7 @@ struct bp_batch {
 };
 
 namespace {
-constexpr int kBatchTilesPerItem = 16;  // 4096-sample work items
+constexpr int kBatchSamplesPerItem = 4096;  // samples per work item
 
 int masked_minmax(const bp::TableView& tv, int P, const uint32_t* mask, int2* out,
                   cudaStream_t st) {
@@ -1120,6 +1186,11 @@ int bp_batch_create(const bp_table* const* tables, int n_tables, const bp_record
   BP_CUDA(cudaGetDevice(&dev));
   retain_pool(dev);
   const int P = tables[0] ? tables[0]->dev.P : 0;
+  int cfg = pick_config(storage, true);
+  for (int i = 0; i < n_tables; ++i)
+    if (tables[i] && tables[i]->info.uses_window_kernel && config_for(tables[i], storage, true) != cfg)
+      cfg = 0;
+  const int tt = cfg_time_tile(cfg);
   int rowcap = 0, max_active = 1;
   bool any_nonfinite = false;
   std::vector<bp::TableView> tv(n_tables);
@@ -1130,7 +1201,7 @@ int bp_batch_create(const bp_table* const* tables, int n_tables, const bp_record
       return fail(BP_ERR_UNSUPPORTED, "table %d needs the direct kernel; batches use the staged one", i);
     if (t->dev.P != P) return fail(BP_ERR_INVALID_ARGUMENT, "tables of a batch share n_phases");
     if (t->device != dev) return fail(BP_ERR_INVALID_ARGUMENT, "table %d is on another device", i);
-    rowcap = std::max(rowcap, rowcap_for(t));
+    rowcap = std::max(rowcap, rowcap_for(t, cfg));
     max_active = std::max(max_active, t->info.max_active);
     any_nonfinite |= t->info.any_nonfinite != 0;
     tv[i] = table_view(t);
@@ -1164,9 +1235,9 @@ int bp_batch_create(const bp_table* const* tables, int n_tables, const bp_record
     v.out1 = (int)q.out1;
     v.flexible = q.out_of_bounds;
     v.table = q.table;
-    v.tpc = kBatchTilesPerItem;
-    const int tau_first = v.out0 / kTimeTile;
-    const int tau_end = (v.out1 + kTimeTile - 1) / kTimeTile;
+    v.tpc = kBatchSamplesPerItem / tt;
+    const int tau_first = v.out0 / tt;
+    const int tau_end = (v.out1 + tt - 1) / tt;
     v.n_chunks = (tau_end - tau_first + v.tpc - 1) / v.tpc;
     v.station_mask = q.station_mask;
     v.beam_max = q.beam_max;
@@ -1181,6 +1252,7 @@ int bp_batch_create(const bp_table* const* tables, int n_tables, const bp_record
   b->storage = storage;
   b->n_records = n_records;
   b->rowcap = rowcap;
+  b->cfg = cfg;
   b->max_active = max_active;
   b->checked = any_flexible && any_nonfinite;
   b->stream = st;
@@ -1258,7 +1330,8 @@ int bp_batch_run(bp_batch* b, void* stream) {
   a.rowcap = b->rowcap;
   a.max_active = b->max_active;
   a.status = b->d_status;
-  if (int rc = launch_window<true>(b->P, b->checked, b->storage, a, true, 0, b->device, st))
+  if (int rc = launch_window<true>(b->cfg, b->P, b->checked, b->storage, a, true, 0, b->device,
+                                   st))
     return rc;
   dim3 grid(64, (unsigned)b->n_records);
   bp::batch_decode_kernel<<<grid, 256, 0, st>>>(b->d_records);
@@ -1317,21 +1390,57 @@ int bp_record_beamform_max_dev(const bp_table* t, const bp_record* q, int storag
   r.out1 = (int)q->out1;
   r.flexible = q->out_of_bounds;
   r.keys = keys;
-  const int tau_first = r.out0 / kTimeTile;
-  const int n_tt = (r.out1 + kTimeTile - 1) / kTimeTile - tau_first;
+  const int cfg = config_for(t, storage, true);
+  const int tt = cfg_time_tile(cfg);
+  const int tau_first = r.out0 / tt;
+  const int n_tt = (r.out1 + tt - 1) / tt - tau_first;
   a.tiles_per_chunk = choose_tiles_per_chunk(n_tt, t->dev.n_tiles, t->device);
-  a.rowcap = rowcap_for(t);
+  a.rowcap = rowcap_for(t, cfg);
   a.max_active = std::max(1, t->info.max_active);
   a.status = t->status;
   const long long blocks =
       (long long)((n_tt + a.tiles_per_chunk - 1) / a.tiles_per_chunk) * t->dev.n_tiles;
   const bool checked = q->out_of_bounds && t->info.any_nonfinite;
-  if (int rc = launch_window<true>(t->dev.P, checked, storage, a, false, blocks, t->device, st))
+  if (int rc = launch_window<true>(cfg, t->dev.P, checked, storage, a, false, blocks, t->device,
+                                   st))
     return rc;
   bp::decode_keys_kernel<<<(unsigned)((n_out + 255) / 256), 256, 0, st>>>(
       keys, (int)n_out, q->beam_max, q->argmax);
   BP_LAUNCHED("decode_keys_kernel");
   return BP_OK;
+}
+
+}  // extern "C"
+
+extern "C" {
+
+int bp_kernel_config_count(void) { return kNumConfigs; }
+
+int bp_kernel_config_describe(int cfg, int* sources_per_thread, int* samples_per_lane,
+                              int* consumer_warps, int* stages) {
+  if (cfg < 0 || cfg >= kNumConfigs) return fail(BP_ERR_INVALID_ARGUMENT, "no config %d", cfg);
+  const int ks = cfg == 1 ? KCfg<1>::KS : KCfg<0>::KS;
+  const int mt = cfg == 1 ? KCfg<1>::MT : KCfg<0>::MT;
+  const int ws = cfg == 1 ? KCfg<1>::WS : KCfg<0>::WS;
+  const int ns = cfg == 1 ? KCfg<1>::NSTAGE : KCfg<0>::NSTAGE;
+  if (sources_per_thread) *sources_per_thread = ks;
+  if (samples_per_lane) *samples_per_lane = mt;
+  if (consumer_warps) *consumer_warps = ws;
+  if (stages) *stages = ns;
+  return BP_OK;
+}
+
+int bp_set_kernel_config(int storage, int reduce, int cfg) {
+  if (storage < 0 || storage > 2 || (reduce != BP_REDUCE_MAX && reduce != BP_REDUCE_NONE))
+    return fail(BP_ERR_INVALID_ARGUMENT, "bad storage / reduce");
+  if (cfg < -1 || cfg >= kNumConfigs) return fail(BP_ERR_INVALID_ARGUMENT, "no config %d", cfg);
+  g_cfg_choice[storage][reduce == BP_REDUCE_MAX ? 1 : 0].store(cfg);
+  return BP_OK;
+}
+
+int bp_get_kernel_config(int storage, int reduce) {
+  if (storage < 0 || storage > 2) return 0;
+  return pick_config(storage, reduce == BP_REDUCE_MAX);
 }
 
 }  // extern "C"

@@ -323,10 +323,6 @@ __device__ __forceinline__ int pair_sample(int lane, int q, int h) {
   else return 2 * lane + 64 * q + h;
 }
 
-#ifndef BP_WINDOW_MIN_BLOCKS
-#define BP_WINDOW_MIN_BLOCKS 2
-#endif
-
 // The staged shift-and-stack for one item (record, source tile, time tiles
 // [tau0, tau1)), shared by the plain and the persistent kernels.
 template <int P, int KS, int MT, int WS, int NSTAGE, bool MAXRED, bool CHECKED, int STORAGE>
@@ -707,8 +703,9 @@ struct Staged {
 // Plain launch: one record, block = (source tile, chunk of time tiles),
 // time-chunk major so that the blocks in flight share an L2-resident stretch
 // of trace.
-template <int P, int KS, int MT, int WS, int NSTAGE, bool MAXRED, bool CHECKED, int STORAGE>
-__global__ void __launch_bounds__((WS + 1) * 32, BP_WINDOW_MIN_BLOCKS)
+template <int P, int KS, int MT, int WS, int NSTAGE, int MINB, bool MAXRED, bool CHECKED,
+          int STORAGE>
+__global__ void __launch_bounds__((WS + 1) * 32, MINB)
 beam_window_kernel(const LaunchArgs a) {
   using St = Staged<P, KS, MT, WS, NSTAGE, MAXRED, CHECKED, STORAGE>;
   extern __shared__ __align__(128) unsigned char smem[];
@@ -730,8 +727,9 @@ beam_window_kernel(const LaunchArgs a) {
 // source tile x a chunk of r.tpc time tiles, time-chunk major).  Records may
 // differ in length, station subset and table; storage, phases and reduce are
 // the launch's.
-template <int P, int KS, int MT, int WS, int NSTAGE, bool MAXRED, bool CHECKED, int STORAGE>
-__global__ void __launch_bounds__((WS + 1) * 32, BP_WINDOW_MIN_BLOCKS)
+template <int P, int KS, int MT, int WS, int NSTAGE, int MINB, bool MAXRED, bool CHECKED,
+          int STORAGE>
+__global__ void __launch_bounds__((WS + 1) * 32, MINB)
 beam_batch_kernel(const LaunchArgs a) {
   using St = Staged<P, KS, MT, WS, NSTAGE, MAXRED, CHECKED, STORAGE>;
   extern __shared__ __align__(128) unsigned char smem[];

@@ -286,6 +286,21 @@ BP_API int bp_beamform_differential_dev(const float *d_traces, size_t n_samples,
                                         size_t n_stations, size_t n_phases, float *d_beam,
                                         void *stream);
 
+/* ---- staged-kernel configurations (autotuning) -------------------------- */
+/* The staged kernel exists in several shapes (sources per thread, samples per
+ * lane, consumer warps, ring stages), all over the same 64-source tables.
+ * bp_set_kernel_config chooses one per (storage, reduce) for every later
+ * launch in the process (-1: built-in default); the environment variable
+ * BEAMPOWER_B200_KERNEL_CONFIG overrides it.  beampower_b200/autotune.py
+ * times the shapes on a workload and stores its choices.  No reference
+ * counterpart (the reference has one launch shape, beamform.cu:10). */
+BP_API int bp_kernel_config_count(void);
+BP_API int bp_kernel_config_describe(int config, int *sources_per_thread,
+                                     int *samples_per_lane, int *consumer_warps,
+                                     int *stages);
+BP_API int bp_set_kernel_config(int storage, int reduce, int config);
+BP_API int bp_get_kernel_config(int storage, int reduce);
+
 /* ---- diagnostics -------------------------------------------------------- */
 /* Last error message of the calling thread ("" if none). */
 BP_API const char *bp_last_error(void);

@@ -115,3 +115,12 @@ def test_key_order_matches_reference_max_rule():
             assert k != 0 and 0xFFFFFFFF - (k & 0xFFFFFFFF) == besti
         else:
             assert k == 0
+
+
+def test_kernel_configs_described():
+    from beampower_b200.autotune import configs
+    cfgs = configs()
+    assert len(cfgs) >= 2
+    for c, d in cfgs:
+        assert d["sources_per_thread"] * d["consumer_warps"] == 64  # the table's tile
+        assert d["samples_per_lane"] % 2 == 0 and d["stages"] >= 2
