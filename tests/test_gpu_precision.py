@@ -90,3 +90,38 @@ def test_16bit_torch_path_and_scales(cuda, orc):
         bm, am = table.beamform_max(tr, 0)
         torch.cuda.synchronize()
     table.close()
+
+
+def test_precision_report(cuda, orc, capsys):
+    """Per-config error statement for 16-bit storage: the 4,000-source
+    network with Gaussian and with heavy-tailed (Student-t, nu = 3) noise,
+    all sources, strict rule; relative error of every computed beam and of
+    beam_max against float64, and argmax agreement above the margin."""
+    import json
+    import beampower_b200 as bp
+    from beampower_b200.synthetic import SMALL, SMALL_HEAVY, make_workload
+    report = []
+    for spec in (SMALL, SMALL_HEAVY):
+        wl = make_workload(spec)
+        F, A, D, W = (wl["waveform_features"], wl["weights_phases"], wl["time_delays"],
+                      wl["weights_sources"])
+        beam64, valid = orc.fp64_beams(orc.fp64_prestack(F, A), D, W, 0)
+        big = valid & (np.abs(beam64) > 1e-6 * np.abs(beam64).max())
+        for storage in ("fp32", "fp16", "bf16"):
+            tol = TOL.get(storage, 1e-5)
+            beam = bp.beamform(F, D, A, W, reduce=None, storage=storage)
+            rel = np.abs(beam[big] - beam64[big]) / np.abs(beam64[big])
+            bm, am = bp.beamform(F, D, A, W, reduce="max", storage=storage)
+            sure, arg64, top1 = _margin_mask(beam64, valid, tol)
+            has = np.isfinite(top1)
+            relm = np.abs(bm[has] - top1[has]) / np.abs(top1[has])
+            row = {"config": spec.name, "storage": storage, "max_rel_beam": float(rel.max()),
+                   "p999_rel_beam": float(np.percentile(rel, 99.9)),
+                   "mean_rel_beam": float(rel.mean()), "max_rel_beam_max": float(relm.max()),
+                   "argmax_above_margin_agree": float(np.mean(am[sure] == arg64[sure])),
+                   "samples_above_margin": int(sure.sum()), "samples": int(has.sum())}
+            report.append(row)
+            assert row["max_rel_beam"] <= tol and row["argmax_above_margin_agree"] == 1.0
+    with capsys.disabled():
+        for row in report:
+            print("PRECISION " + json.dumps(row))
