@@ -1444,3 +1444,41 @@ int bp_get_kernel_config(int storage, int reduce) {
 }
 
 }  // extern "C"
+
+namespace {
+// A wait that can never complete: an mbarrier expecting one arrival that no
+// thread makes.  Every thread gives up after `limit_ns` and the kernel ends.
+__global__ void wait_timeout_probe_kernel(unsigned long long limit_ns, int* status) {
+  __shared__ uint64_t bar;
+  if (threadIdx.x == 0) {
+    bp::mbar_init(&bar, 1);
+    bp::fence_mbar_init();
+  }
+  __syncthreads();
+  bp::mbar_wait_limit(&bar, 0, limit_ns, status);
+}
+}  // namespace
+
+extern "C" {
+
+int bp_debug_wait_timeout(unsigned long long limit_ns, void* stream, int* status_out) {
+  g_last_error.clear();
+  if (!status_out) return fail(BP_ERR_INVALID_ARGUMENT, "NULL status");
+  if (limit_ns > 1000000000ull) return fail(BP_ERR_INVALID_ARGUMENT, "limit above 1 s");
+  cudaStream_t st = as_stream(stream);
+  int* d = nullptr;
+  BP_CUDA(cudaMallocAsync(&d, sizeof(int), st));
+  cudaError_t e = cudaMemsetAsync(d, 0, sizeof(int), st);
+  if (e == cudaSuccess) {
+    wait_timeout_probe_kernel<<<1, 64, 0, st>>>(limit_ns, d);
+    g_launches.fetch_add(1);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(status_out, d, sizeof(int), cudaMemcpyDeviceToHost, st);
+  cudaFreeAsync(d, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return cuda_fail(e, "wait timeout probe");
+  return BP_OK;
+}
+
+}  // extern "C"

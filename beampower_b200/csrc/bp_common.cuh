@@ -140,6 +140,19 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
   }
 }
 
+// Same with a caller-given limit (diagnostics).
+__device__ __forceinline__ bool mbar_wait_limit(uint64_t* bar, uint32_t parity,
+                                                unsigned long long limit_ns, int* status) {
+  const unsigned long long start = globaltimer_ns();
+  while (!mbar_try_wait(bar, parity)) {
+    if (globaltimer_ns() - start > limit_ns) {
+      if (status) atomicOr(status, kStatusWaitTimeout);
+      return false;
+    }
+  }
+  return true;
+}
+
 // 1-D bulk copy global -> shared through the TMA engine, completing on an
 // mbarrier.  Both addresses 16-byte aligned, size a multiple of 16 bytes.
 // No multicast: every copy reads this GPU's own memory into this CTA.

@@ -34,6 +34,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+from beampower_b200.replicas import barrier, max_over_ranks  # noqa: E402
 from beampower_b200.synthetic import LARGE, make_workload, nominal_terms  # noqa: E402
 
 MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
@@ -304,7 +305,7 @@ def run_ours(args, rank, world, local_rank):
     if dist:
         import torch.distributed as tdist
         from datetime import timedelta
-        tdist.init_process_group("nccl", timeout=timedelta(seconds=300))
+        tdist.init_process_group("nccl", timeout=timedelta(seconds=120))
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
     lib = load_library("gpu")
@@ -354,8 +355,7 @@ def run_ours(args, rank, world, local_rank):
     recs = []
     launches0 = lib.bp_launch_count()
     sampler = ClockSampler(local_rank) if rank == 0 else None
-    if dist:
-        tdist.barrier()
+    barrier(dev)
     torch.cuda.synchronize()
     if sampler:
         sampler.start()
@@ -369,17 +369,31 @@ def run_ours(args, rank, world, local_rank):
     clocks = sampler.stop() if sampler else None
     launches = lib.bp_launch_count() - launches0
     elapsed_ms = t_start.elapsed_time(t_end)
-    if dist:
-        t = torch.tensor([elapsed_ms], device=dev)
-        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
-        elapsed_ms = float(t.item())
+    elapsed_ms = max_over_ranks(elapsed_ms, dev)
     table_ms = statistics.mean(r[0].elapsed_time(r[1]) for r in recs)
     prestack_ms = statistics.mean(r[1].elapsed_time(r[2]) for r in recs)
     kernel_ms = statistics.mean(r[2].elapsed_time(r[3]) for r in recs)
     info = recs[0][4].info
-    # parity spot check of the last step at a few samples (cheap, GPU only):
-    # the argmax sources' beams are recomputed by the direct kernel elsewhere.
-    bm_last = recs[-1][6]
+    # the other trace storage types on the same resident table (kernel only)
+    variants = {}
+    if not args.profile:
+        vt = recs[-1][4]
+        for stg in ("fp32", "fp16", "bf16"):
+            if stg == args.storage:
+                continue
+            tr = vt.traces_from_features(dF, dA, storage=stg)
+            vt.beamform_max(tr, oob)
+            e0, e1 = ev(), ev()
+            e0.record(stream)
+            for _ in range(2):
+                vt.beamform_max(tr, oob)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            kms = e0.elapsed_time(e1) / 2
+            variants[stg] = {"kernel_ms": kms, "value": terms / (kms * 1e-3),
+                             "unit": "beam terms/s", "kernel_config":
+                             lib.bp_get_kernel_config({"fp32": 0, "bf16": 1, "fp16": 2}[stg], 1)}
+            del tr
     for r in recs:
         r[4].close()
     ms_per_step = elapsed_ms / args.steps
@@ -403,18 +417,14 @@ def run_ours(args, rank, world, local_rank):
                 storage=args.storage)
     e2e_times = []
     for _ in range(max(2, min(args.steps, 3))):
-        if dist:
-            tdist.barrier()
+        barrier(dev)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         bp.beamform(hF, hD, hA, hW, reduce="max", out_of_bounds=args.out_of_bounds,
                     storage=args.storage)
         e2e_times.append(time.perf_counter() - t0)
     e2e_s = statistics.mean(e2e_times)
-    if dist:
-        t = torch.tensor([e2e_s], device=dev)
-        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks(e2e_s, dev)
     h2d = F.nbytes + A.nbytes + D.nbytes + W.nbytes
     d2h = 8 * T
 
@@ -469,6 +479,7 @@ def run_ours(args, rank, world, local_rank):
                              "peak_gbs": hbm_peak, "of": "measured (MEASURED_PEAKS.json)"},
             },
             "table": info,
+            "storage_variants": variants,
             "e2e": {"value": world * terms / e2e_s, "unit": "beam terms/s",
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "seconds_per_step": e2e_s},
@@ -476,7 +487,7 @@ def run_ours(args, rank, world, local_rank):
             "clocks": clocks,
         }
     if dist:
-        tdist.barrier()
+        barrier(dev)
         tdist.destroy_process_group()
     if rank != 0:
         return

@@ -308,6 +308,12 @@ BP_API const char *bp_last_error(void);
  * FP32 FMA throughput (TFLOP/s) with short microbenchmarks on `stream`
  * (synchronises it).  These are the rooflines of the staged kernel. */
 BP_API int bp_measure_peaks(void *stream, double *smem_gbs, double *fp32_tflops);
+/* Failure-path check: launches a kernel whose threads wait on an mbarrier
+ * that nothing completes, with a limit of limit_ns (at most 1 s); the wait
+ * gives up, the kernel ends, and *status_out receives the status bits
+ * (1 = wait timeout).  Shows that a wait which can never finish ends with an
+ * error status instead of hanging the GPU.  Synchronises `stream`. */
+BP_API int bp_debug_wait_timeout(unsigned long long limit_ns, void *stream, int *status_out);
 /* Library version string. */
 BP_API const char *bp_version(void);
 /* Kernel launches issued by this process since load (all entry points). */
