@@ -17,7 +17,7 @@ INCLUDE = os.path.join(ROOT, "include")
 LIBDIR = os.path.join(PKG, "lib")
 LIB = os.path.join(LIBDIR, "libbeampower_b200.so")
 
-NVCC_FLAGS = [
+COMPILE_FLAGS = [
     "-O3",
     "-std=c++17",
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -25,6 +25,9 @@ NVCC_FLAGS = [
     "-Xcompiler", "-fPIC",
     "-Xcompiler", "-fvisibility=hidden",
     "--expt-relaxed-constexpr",
+]
+LINK_FLAGS = [
+    "-gencode", "arch=compute_100a,code=sm_100a",
     "-shared",
     "-cudart", "static",
 ]
@@ -53,20 +56,49 @@ def nvcc() -> str:
     return "nvcc"
 
 
-def build(force: bool = False, verbose: bool = False, extra=()) -> str:
-    """Compile every .cu under csrc/ into one shared library; return its path."""
+def _host_compiler():
+    # nvcc's host compiler: the system gcc (the image's CC wrapper is incomplete)
+    return ["-ccbin", "/usr/bin/g++"] if os.path.exists("/usr/bin/gcc") else []
+
+
+def build(force: bool = False, verbose: bool = False, extra=(), jobs=None) -> str:
+    """Compile every .cu under csrc/ (one nvcc per file, in parallel) and link
+    them into one shared library; return its path."""
     if not force and up_to_date():
         return LIB
     os.makedirs(LIBDIR, exist_ok=True)
+    objdir = os.path.join(LIBDIR, "obj")
+    os.makedirs(objdir, exist_ok=True)
+    cc = _host_compiler()
+    jobs = jobs or max(1, min(len(sources()), os.cpu_count() or 1))
+
+    def compile_one(src):
+        obj = os.path.join(objdir, os.path.basename(src)[:-3] + ".o")
+        cmd = [nvcc(), *cc, *COMPILE_FLAGS, *extra, "-I", INCLUDE, "-I", CSRC, "-c", src,
+               "-o", obj]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        return src, obj, r
+
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(max_workers=jobs) as ex:
+        results = list(ex.map(compile_one, sources()))
+    failed = False
+    for src, _obj, r in results:
+        if r.stdout or r.stderr:
+            sys.stdout.write(r.stdout)
+            sys.stderr.write(r.stderr)
+        if r.returncode != 0:
+            failed = True
+            sys.stderr.write(f"nvcc failed on {src}\n")
+    if failed:
+        raise subprocess.CalledProcessError(1, "nvcc")
     tmp = LIB + ".tmp"
-    cmd = [nvcc(), *NVCC_FLAGS, *extra, "-I", INCLUDE, "-I", CSRC, *sources(), "-o", tmp]
-    env = dict(os.environ)
-    # nvcc's host compiler: the system gcc (the image's CC wrapper is incomplete)
-    if os.path.exists("/usr/bin/gcc"):
-        cmd[1:1] = ["-ccbin", "/usr/bin/g++"]
+    cmd = [nvcc(), *cc, *LINK_FLAGS, *(obj for _s, obj, _r in results), "-o", tmp]
     if verbose:
-        print(" ".join(cmd))
-    subprocess.run(cmd, check=True, env=env)
+        print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
     os.replace(tmp, LIB)
     return LIB
 

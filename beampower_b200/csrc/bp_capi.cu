@@ -16,8 +16,9 @@
 #include "beampower_b200.h"
 #include "bp_common.cuh"
 #include "bp_kernels.cuh"
+#include "bp_host.h"
 
-namespace {
+namespace bp_host {
 
 thread_local std::string g_last_error;
 std::atomic<uint64_t> g_launches{0};
@@ -38,44 +39,44 @@ int cuda_fail(cudaError_t e, const char* what) {
   return fail(BP_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
 }
 
-#define BP_CUDA(call)                                  \
-  do {                                                 \
-    cudaError_t e_ = (call);                           \
-    if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
-  } while (0)
+int device_sm_count(int dev) {
+  static int cache[64] = {0};
+  if (dev >= 0 && dev < 64 && cache[dev]) return cache[dev];
+  int v = 0;
+  cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+  if (dev >= 0 && dev < 64) cache[dev] = v;
+  return v;
+}
 
-#define BP_LAUNCHED(what)                                         \
-  do {                                                            \
-    g_launches.fetch_add(1, std::memory_order_relaxed);           \
-    cudaError_t e_ = cudaGetLastError();                          \
-    if (e_ != cudaSuccess) return cuda_fail(e_, "launch " what);   \
-  } while (0)
+int device_smem_optin(int dev) {
+  static int cache[64] = {0};
+  if (dev >= 0 && dev < 64 && cache[dev]) return cache[dev];
+  int v = 0;
+  cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  if (dev >= 0 && dev < 64) cache[dev] = v;
+  return v;
+}
+
+}  // namespace bp_host
+
+using namespace bp_host;
+
+namespace {
 
 inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 
-constexpr long long kMaxInt = std::numeric_limits<int>::max();
-
-// ---- staged-kernel configurations --------------------------------------------
-// All use 64-source tiles (the table's tile size).  Config 0: 8 consumer warps
-// x 8 sources per thread, 8 samples per lane (256-sample time tiles), 2 blocks
-// per SM.  Config 1: 16 consumer warps x 4 sources, 16 samples per lane
-// (512-sample time tiles), 1 block per SM: twice the terms per metadata load.
-#ifndef BP_NSTAGE
-#define BP_NSTAGE 4
-#endif
-template <int ID> struct KCfg;
-template <> struct KCfg<0> {
-  static constexpr int KS = 8, MT = 8, WS = 8, NSTAGE = BP_NSTAGE, MINB = 2;
+struct CfgDesc {
+  int ks, mt, ws, nstage;
 };
-template <> struct KCfg<1> {
-  static constexpr int KS = 4, MT = 16, WS = 16, NSTAGE = BP_NSTAGE, MINB = 1;
-};
-constexpr int kNumConfigs = 2;
-constexpr int kTileSources = 64;
-static_assert(KCfg<0>::KS * KCfg<0>::WS == kTileSources, "tile size");
-static_assert(KCfg<1>::KS * KCfg<1>::WS == kTileSources, "tile size");
+template <int ID>
+constexpr CfgDesc cfg_desc() {
+  return {KCfg<ID>::KS, KCfg<ID>::MT, KCfg<ID>::WS, KCfg<ID>::NSTAGE};
+}
+constexpr CfgDesc kCfgDesc[kNumConfigs] = {cfg_desc<0>(), cfg_desc<1>()};
 
-inline int cfg_time_tile(int cfg) { return cfg == 1 ? 32 * KCfg<1>::MT : 32 * KCfg<0>::MT; }
+inline int cfg_time_tile(int cfg) {
+  return 32 * kCfgDesc[(cfg >= 0 && cfg < kNumConfigs) ? cfg : 0].mt;
+}
 
 // Preferred config per (storage, reduce); -1 = built-in default.
 std::atomic<int> g_cfg_choice[3][2] = {{{-1}, {-1}}, {{-1}, {-1}}, {{-1}, {-1}}};
@@ -93,24 +94,6 @@ int pick_config(int storage, bool maxred) {
   // FP32 storage is shared-memory bound and favours config 0; 16-bit storage
   // is issue bound and gains from config 1's longer time tiles.
   return storage == BP_STORAGE_F32 ? 0 : 1;
-}
-
-int device_sm_count(int dev) {
-  static int cache[64] = {0};
-  if (dev >= 0 && dev < 64 && cache[dev]) return cache[dev];
-  int v = 0;
-  cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
-  if (dev >= 0 && dev < 64) cache[dev] = v;
-  return v;
-}
-
-int device_smem_optin(int dev) {
-  static int cache[64] = {0};
-  if (dev >= 0 && dev < 64 && cache[dev]) return cache[dev];
-  int v = 0;
-  cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-  if (dev >= 0 && dev < 64) cache[dev] = v;
-  return v;
 }
 
 }  // namespace
@@ -279,68 +262,6 @@ int build_tiling_map(const int32_t* d_delays, const float* d_w, size_t N, size_t
   return rc;
 }
 
-// ---- staged kernel dispatch -------------------------------------------------
-template <int CFG, int P, bool MAXRED, bool CHECKED, int STORAGE>
-int launch_window_p(const bp::LaunchArgs& a, bool batch, long long plain_blocks, int dev,
-                    cudaStream_t st) {
-  using C = KCfg<CFG>;
-  using L = bp::WindowSmem<P, C::KS, C::MT, C::WS, C::NSTAGE, MAXRED>;
-  const L lay(a.rowcap, a.max_active);
-  if (lay.total > (size_t)device_smem_optin(dev))
-    return fail(BP_ERR_UNSUPPORTED, "staged kernel needs %zu B of shared memory", lay.total);
-  constexpr int threads = bp::WindowCfg<P, C::KS, C::MT, C::WS>::kThreads;
-  if (batch) {
-    auto kern = bp::beam_batch_kernel<P, C::KS, C::MT, C::WS, C::NSTAGE, C::MINB, MAXRED,
-                                      CHECKED, STORAGE>;
-    BP_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)lay.total));
-    int per_sm = 0;
-    BP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, lay.total));
-    const int grid = std::max(1, per_sm) * std::max(1, device_sm_count(dev));
-    kern<<<grid, threads, lay.total, st>>>(a);
-    BP_LAUNCHED("beam_batch_kernel");
-  } else {
-    auto kern = bp::beam_window_kernel<P, C::KS, C::MT, C::WS, C::NSTAGE, C::MINB, MAXRED,
-                                       CHECKED, STORAGE>;
-    BP_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)lay.total));
-    if (plain_blocks > kMaxInt) return fail(BP_ERR_UNSUPPORTED, "grid too large");
-    if (plain_blocks <= 0) return BP_OK;
-    kern<<<(unsigned)plain_blocks, threads, lay.total, st>>>(a);
-    BP_LAUNCHED("beam_window_kernel");
-  }
-  return BP_OK;
-}
-
-template <int CFG, bool MAXRED, bool CHECKED, int STORAGE>
-int launch_window_s(int P, const bp::LaunchArgs& a, bool batch, long long blocks, int dev,
-                    cudaStream_t st) {
-  switch (P) {
-    case 1: return launch_window_p<CFG, 1, MAXRED, CHECKED, STORAGE>(a, batch, blocks, dev, st);
-    case 2: return launch_window_p<CFG, 2, MAXRED, CHECKED, STORAGE>(a, batch, blocks, dev, st);
-    case 3: return launch_window_p<CFG, 3, MAXRED, CHECKED, STORAGE>(a, batch, blocks, dev, st);
-    case 4: return launch_window_p<CFG, 4, MAXRED, CHECKED, STORAGE>(a, batch, blocks, dev, st);
-    default: return fail(BP_ERR_UNSUPPORTED, "staged kernel supports 1..4 phases");
-  }
-}
-
-template <int CFG, bool MAXRED>
-int launch_window_c(int P, bool checked, int storage, const bp::LaunchArgs& a, bool batch,
-                    long long blocks, int dev, cudaStream_t st) {
-  if (storage == BP_STORAGE_F32)
-    return checked
-               ? launch_window_s<CFG, MAXRED, true, BP_STORAGE_F32>(P, a, batch, blocks, dev, st)
-               : launch_window_s<CFG, MAXRED, false, BP_STORAGE_F32>(P, a, batch, blocks, dev, st);
-  if (checked)
-    return fail(BP_ERR_UNSUPPORTED,
-                "non-finite weights in flexible mode need FP32 trace storage");
-  if (storage == BP_STORAGE_BF16)
-    return launch_window_s<CFG, MAXRED, false, BP_STORAGE_BF16>(P, a, batch, blocks, dev, st);
-  if (storage == BP_STORAGE_F16)
-    return launch_window_s<CFG, MAXRED, false, BP_STORAGE_F16>(P, a, batch, blocks, dev, st);
-  return fail(BP_ERR_INVALID_ARGUMENT, "unknown storage %d", storage);
-}
-
 template <bool MAXRED>
 int launch_window(int cfg, int P, bool checked, int storage, const bp::LaunchArgs& a,
                   bool batch, long long blocks, int dev, cudaStream_t st) {
@@ -368,8 +289,8 @@ size_t staged_smem_cfg(int P, bool maxred, int rowcap, int max_active) {
 }
 
 size_t staged_smem_bytes(int cfg, int P, bool maxred, int rowcap, int max_active) {
-  return cfg == 1 ? staged_smem_cfg<1>(P, maxred, rowcap, max_active)
-                  : staged_smem_cfg<0>(P, maxred, rowcap, max_active);
+  if (cfg == 1) return staged_smem_cfg<1>(P, maxred, rowcap, max_active);
+  return staged_smem_cfg<0>(P, maxred, rowcap, max_active);
 }
 
 int rowcap_for(const bp_table* t, int cfg) {
@@ -1419,14 +1340,11 @@ int bp_kernel_config_count(void) { return kNumConfigs; }
 int bp_kernel_config_describe(int cfg, int* sources_per_thread, int* samples_per_lane,
                               int* consumer_warps, int* stages) {
   if (cfg < 0 || cfg >= kNumConfigs) return fail(BP_ERR_INVALID_ARGUMENT, "no config %d", cfg);
-  const int ks = cfg == 1 ? KCfg<1>::KS : KCfg<0>::KS;
-  const int mt = cfg == 1 ? KCfg<1>::MT : KCfg<0>::MT;
-  const int ws = cfg == 1 ? KCfg<1>::WS : KCfg<0>::WS;
-  const int ns = cfg == 1 ? KCfg<1>::NSTAGE : KCfg<0>::NSTAGE;
-  if (sources_per_thread) *sources_per_thread = ks;
-  if (samples_per_lane) *samples_per_lane = mt;
-  if (consumer_warps) *consumer_warps = ws;
-  if (stages) *stages = ns;
+  const CfgDesc& d = kCfgDesc[cfg];
+  if (sources_per_thread) *sources_per_thread = d.ks;
+  if (samples_per_lane) *samples_per_lane = d.mt;
+  if (consumer_warps) *consumer_warps = d.ws;
+  if (stages) *stages = d.nstage;
   return BP_OK;
 }
 

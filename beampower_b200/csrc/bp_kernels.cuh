@@ -772,6 +772,9 @@ beam_batch_kernel(const LaunchArgs a) {
   }
 }
 
+// Everything below holds non-template kernels (one definition per program), so
+// the files that only instantiate the staged kernel leave it out.
+#ifndef BP_STAGED_KERNELS_ONLY
 
 // Decode every record's keys of a batch into its outputs.
 __global__ void batch_decode_kernel(const RecordView* __restrict__ recs) {
@@ -1182,5 +1185,7 @@ __global__ void prestack_h16_kernel(const float* __restrict__ F, const float* __
     }
   }
 }
+
+#endif  // BP_STAGED_KERNELS_ONLY
 
 }  // namespace bp
