@@ -90,6 +90,12 @@ SIGNATURES = {
     "beamform_differential": ([_f32p, _i32p, _f32p, _sz, _sz, _sz, _sz, _int, _f32p], _int),
     "bp_beamform_differential_dev": ([_vp, _sz, _sz, _sz, _vp, _vp, _sz, _sz, _sz, _vp, _vp],
                                      _int),
+    "bp_threshold_dev": ([_vp, _sz, _sz, ct.c_double, _int, ct.c_float, _vp, _sz,
+                          ct.c_ulonglong, _vp, _vp], _int),
+    "bp_find_peaks_dev": ([_vp, _sz, ct.c_double, _vp, _sz, ct.POINTER(_sz), _vp], _int),
+    "bp_detect_dev": ([_vp, _vp, _vp, _sz, ct.c_double, _vp, _vp, _vp, _sz, ct.POINTER(_sz),
+                       _vp], _int),
+    "bp_pairwise_sum_f32": ([_vp, _sz], ct.c_float),
     "bp_measure_peaks": ([_vp, ct.POINTER(ct.c_double), ct.POINTER(ct.c_double)], _int),
     "bp_beamform_max_noalloc": ([_vp, _sz, _sz, _sz, _vp, _vp, _sz, _sz, _sz, _int, _vp, _vp,
                                  _vp], _int),

@@ -1,0 +1,924 @@
+// Detection on the beam series, on the GPU: the reference tutorial's
+// time-dependent threshold (notebooks/3_beampower.ipynb:497-579) and its
+// peak picking -- scipy.signal.find_peaks(beam_max, distance=...) followed by
+// the strict threshold test (notebooks/3_beampower.ipynb:618-626) -- with
+// results identical to the NumPy / SciPy code.
+//
+// Exactness rests on three restatements:
+//  * NumPy's float32 sum (inside mean and std) is a pairwise sum whose split
+//    points depend on the length only.  The split tree is built on the host;
+//    its leaves are summed in parallel and its inner nodes level by level,
+//    each with the same rounded operations as NumPy's loop.
+//  * NumPy's median is an order statistic (the mean of the two middle values
+//    for even lengths); a 4-pass 8-bit radix select on the order-preserving
+//    integer image of the floats finds it exactly.
+//  * SciPy's distance rule is a greedy pass in decreasing height.  Its result
+//    is also the fixed point of rounds in which every undecided peak with no
+//    higher undecided peak within the distance is kept, and then every
+//    undecided peak within the distance of a kept one is dropped.
+#define BP_TEMPLATE_KERNELS_ONLY
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <cstdint>
+#include <vector>
+
+#include <cub/device/device_scan.cuh>
+#include <cuda_runtime.h>
+
+#include "beampower_b200.h"
+#include "bp_host.h"
+
+using namespace bp_host;
+
+namespace {
+
+constexpr unsigned kFull = 0xFFFFFFFFu;
+
+// ---- stream-ordered scratch, freed at scope exit -----------------------------
+struct Scratch {
+  cudaStream_t st;
+  std::vector<void*> ptrs;
+  explicit Scratch(cudaStream_t s) : st(s) {}
+  ~Scratch() {
+    for (void* p : ptrs) cudaFreeAsync(p, st);
+  }
+  template <class T>
+  int get(T** out, size_t count) {
+    void* p = nullptr;
+    cudaError_t e = cudaMallocAsync(&p, std::max<size_t>(count, 1) * sizeof(T), st);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMallocAsync (detection scratch)");
+    ptrs.push_back(p);
+    *out = static_cast<T*>(p);
+    return BP_OK;
+  }
+};
+
+#define BP_TRY(expr)              \
+  do {                            \
+    if (int rc_ = (expr)) return rc_; \
+  } while (0)
+
+template <class T>
+int read_back(T* host, const T* dev, cudaStream_t st) {
+  BP_CUDA(cudaMemcpyAsync(host, dev, sizeof(T), cudaMemcpyDeviceToHost, st));
+  BP_CUDA(cudaStreamSynchronize(st));
+  return BP_OK;
+}
+
+inline unsigned grid_for(long long n, int threads, long long cap = 0x7FFFFFFFLL) {
+  return (unsigned)std::max<long long>(1, std::min<long long>((n + threads - 1) / threads, cap));
+}
+
+// ---- NumPy's float32 pairwise summation --------------------------------------
+// numpy/_core/src/umath/loops_utils.h.src, pairwise_sum: a run of n values
+// sums as: n < 8, in order; n <= 128, eight strided partial sums r[0..7]
+// combined as ((r0+r1)+(r2+r3))+((r4+r5)+(r6+r7)) and then the n % 8 tail in
+// order; otherwise sum([0, n2)) + sum([n2, n)) with n2 = n/2 - (n/2) % 8.
+// The reduction then adds that sum to its initial +0.0.
+constexpr int kPwLeaf = 128;
+
+__host__ __device__ inline float add_rn(float a, float b) {
+#ifdef __CUDA_ARCH__
+  return __fadd_rn(a, b);
+#else
+  return a + b;
+#endif
+}
+
+template <class Get>
+__host__ __device__ inline float pw_leaf(const Get& get, int len) {
+  if (len < 8) {
+    float r = 0.0f;
+    for (int i = 0; i < len; ++i) r = add_rn(r, get(i));
+    return r;
+  }
+  float r0 = get(0), r1 = get(1), r2 = get(2), r3 = get(3);
+  float r4 = get(4), r5 = get(5), r6 = get(6), r7 = get(7);
+  int i = 8;
+  const int lim = len - len % 8;
+  for (; i < lim; i += 8) {
+    r0 = add_rn(r0, get(i + 0));
+    r1 = add_rn(r1, get(i + 1));
+    r2 = add_rn(r2, get(i + 2));
+    r3 = add_rn(r3, get(i + 3));
+    r4 = add_rn(r4, get(i + 4));
+    r5 = add_rn(r5, get(i + 5));
+    r6 = add_rn(r6, get(i + 6));
+    r7 = add_rn(r7, get(i + 7));
+  }
+  float res = add_rn(add_rn(add_rn(r0, r1), add_rn(r2, r3)), add_rn(add_rn(r4, r5), add_rn(r6, r7)));
+  for (; i < len; ++i) res = add_rn(res, get(i));
+  return res;
+}
+
+// The split tree of a length: leaves {node, begin, len}, inner nodes
+// {node, left, right} grouped by height (children always lower).
+struct PwTree {
+  std::vector<int4> leaves;
+  std::vector<int4> inner;
+  std::vector<int> level_end;
+  int n_nodes = 0;
+  int root = 0;
+};
+
+int pw_build(int begin, int len, std::vector<int4>& leaves, std::vector<int4>& inner,
+             std::vector<int>& height, int& next_id, int* h_out) {
+  if (len <= kPwLeaf) {
+    const int id = next_id++;
+    leaves.push_back(make_int4(id, begin, len, 0));
+    *h_out = 0;
+    return id;
+  }
+  int n2 = len / 2;
+  n2 -= n2 % 8;
+  int hl = 0, hr = 0;
+  const int l = pw_build(begin, n2, leaves, inner, height, next_id, &hl);
+  const int r = pw_build(begin + n2, len - n2, leaves, inner, height, next_id, &hr);
+  const int id = next_id++;
+  inner.push_back(make_int4(id, l, r, 0));
+  height.push_back(1 + std::max(hl, hr));
+  *h_out = height.back();
+  return id;
+}
+
+PwTree pw_tree(int n) {
+  PwTree t;
+  std::vector<int4> raw;
+  std::vector<int> h;
+  int next = 0, top = 0;
+  t.root = pw_build(0, n, t.leaves, raw, h, next, &top);
+  t.n_nodes = next;
+  std::vector<std::vector<int4>> by_level(top + 1);
+  for (size_t i = 0; i < raw.size(); ++i) by_level[h[i]].push_back(raw[i]);
+  for (int lv = 1; lv <= top; ++lv) {
+    t.inner.insert(t.inner.end(), by_level[lv].begin(), by_level[lv].end());
+    t.level_end.push_back((int)t.inner.size());
+  }
+  return t;
+}
+
+// NumPy divides a float32 sum by its integer count in float64 and stores the
+// quotient as float32 (the count is a NumPy integer, which promotes).
+__device__ __forceinline__ float np_divide_count(float s, int count) {
+  return __double2float_rn(__ddiv_rn((double)s, (double)count));
+}
+
+// Leaves of every segment w (data x + w * seg_stride): mode 0 sums x, mode 1
+// sums (x - centre[w])^2 with NumPy's float32 subtract and multiply.
+__global__ void pw_leaves_kernel(const float* __restrict__ x, long long seg_stride, int mode,
+                                 const float* __restrict__ centre, const int4* __restrict__ leaves,
+                                 int n_leaves, int n_nodes, int n_seg, float* __restrict__ vals) {
+  const int l = blockIdx.x * blockDim.x + threadIdx.x;
+  if (l >= n_leaves) return;
+  const int4 lf = leaves[l];
+  for (int w = blockIdx.y; w < n_seg; w += gridDim.y) {
+    const float* base = x + (size_t)w * seg_stride + lf.y;
+    float s;
+    if (mode == 0) {
+      s = pw_leaf([&](int i) { return base[i]; }, lf.z);
+    } else {
+      const float c = centre[w];
+      s = pw_leaf(
+          [&](int i) {
+            const float d = __fsub_rn(base[i], c);
+            return __fmul_rn(d, d);
+          },
+          lf.z);
+    }
+    vals[(size_t)w * n_nodes + lf.x] = s;
+  }
+}
+
+// Inner nodes of every segment, one block per segment, level by level; then
+// out[w] = (0 + root) / count as NumPy's mean / var store it.
+__global__ void pw_inner_kernel(const int4* __restrict__ inner, const int* __restrict__ level_end,
+                                int n_levels, int n_nodes, int root, int count, int n_seg,
+                                float* __restrict__ vals, float* __restrict__ out) {
+  for (int w = blockIdx.x; w < n_seg; w += gridDim.x) {
+    float* v = vals + (size_t)w * n_nodes;
+    int begin = 0;
+    for (int lv = 0; lv < n_levels; ++lv) {
+      const int end = level_end[lv];
+      for (int i = begin + threadIdx.x; i < end; i += blockDim.x) {
+        const int4 nd = inner[i];
+        v[nd.x] = __fadd_rn(v[nd.y], v[nd.z]);
+      }
+      begin = end;
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) out[w] = np_divide_count(__fadd_rn(0.0f, v[root]), count);
+    __syncthreads();
+  }
+}
+
+// out[w] = mean (mode 0) or population variance (mode 1, given the means) of
+// segments of `len` values starting every seg_stride values.
+int pw_mean(const float* x, long long seg_stride, int len, int n_seg, int mode,
+            const float* centre, float* out, Scratch& sc, cudaStream_t st) {
+  const PwTree t = pw_tree(len);
+  int4 *d_leaves = nullptr, *d_inner = nullptr;
+  int* d_levels = nullptr;
+  float* vals = nullptr;
+  BP_TRY(sc.get(&d_leaves, t.leaves.size()));
+  BP_TRY(sc.get(&d_inner, t.inner.size()));
+  BP_TRY(sc.get(&d_levels, t.level_end.size()));
+  BP_TRY(sc.get(&vals, (size_t)t.n_nodes * n_seg));
+  BP_CUDA(cudaMemcpyAsync(d_leaves, t.leaves.data(), t.leaves.size() * sizeof(int4),
+                          cudaMemcpyHostToDevice, st));
+  if (!t.inner.empty()) {
+    BP_CUDA(cudaMemcpyAsync(d_inner, t.inner.data(), t.inner.size() * sizeof(int4),
+                            cudaMemcpyHostToDevice, st));
+    BP_CUDA(cudaMemcpyAsync(d_levels, t.level_end.data(), t.level_end.size() * sizeof(int),
+                            cudaMemcpyHostToDevice, st));
+  }
+  const int nl = (int)t.leaves.size();
+  dim3 g1((nl + 127) / 128, (unsigned)std::min(n_seg, 65535));
+  pw_leaves_kernel<<<g1, 128, 0, st>>>(x, seg_stride, mode, centre, d_leaves, nl, t.n_nodes,
+                                       n_seg, vals);
+  BP_LAUNCHED("pw_leaves_kernel");
+  pw_inner_kernel<<<(unsigned)std::min(n_seg, 65535), 256, 0, st>>>(
+      d_inner, d_levels, (int)t.level_end.size(), t.n_nodes, t.root, len, n_seg, vals, out);
+  BP_LAUNCHED("pw_inner_kernel");
+  return BP_OK;
+}
+
+// ---- exact medians by radix select -----------------------------------------
+__device__ __forceinline__ uint32_t order_key(float v) {
+  const uint32_t u = __float_as_uint(v);
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float key_float(uint32_t k) {
+  return __uint_as_float((k & 0x80000000u) ? (k & 0x7FFFFFFFu) : ~k);
+}
+
+struct SelState {
+  uint32_t prefix[2];  // decided high bits of the order statistics
+  uint32_t rank[2];    // rank still to find below the decided prefix
+  uint32_t nan;        // NaN count (NumPy's median is NaN if any)
+  int32_t q;           // 1: odd length (one statistic), 2: even (two)
+};
+
+__global__ void select_init_kernel(SelState* st, int n_seg, int len) {
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= n_seg) return;
+  SelState s;
+  s.nan = 0;
+  s.prefix[0] = s.prefix[1] = 0;
+  if (len % 2) {
+    s.q = 1;
+    s.rank[0] = s.rank[1] = (uint32_t)(len / 2);
+  } else {
+    s.q = 2;
+    s.rank[0] = (uint32_t)(len / 2 - 1);
+    s.rank[1] = (uint32_t)(len / 2);
+  }
+  st[w] = s;
+}
+
+// Histogram of the next 8 bits of the values whose higher bits match each
+// statistic's prefix.  mode 1 selects among |x - centre[w]| (float32).
+__global__ void __launch_bounds__(256)
+select_hist_kernel(const float* __restrict__ x, long long seg_stride, int len, int mode,
+                   const float* __restrict__ centre, int n_seg, int pass,
+                   SelState* __restrict__ st, unsigned* __restrict__ hist) {
+  __shared__ unsigned h[2][256];
+  __shared__ unsigned nan_count;
+  const int shift = 24 - 8 * pass;
+  const uint32_t mask = pass == 0 ? 0u : (0xFFFFFFFFu << (32 - 8 * pass));
+  for (int w = blockIdx.y; w < n_seg; w += gridDim.y) {
+    for (int b = threadIdx.x; b < 512; b += blockDim.x) (&h[0][0])[b] = 0;
+    if (threadIdx.x == 0) nan_count = 0;
+    __syncthreads();
+    const int q = st[w].q;
+    const uint32_t p0 = st[w].prefix[0] & mask, p1 = st[w].prefix[1] & mask;
+    const float c = mode ? centre[w] : 0.0f;
+    const float* base = x + (size_t)w * seg_stride;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < len;
+         i += (long long)gridDim.x * blockDim.x) {
+      float v = base[i];
+      if (mode) v = fabsf(__fsub_rn(v, c));
+      if (pass == 0 && isnan(v)) atomicAdd(&nan_count, 1u);
+      const uint32_t key = order_key(v);
+      const uint32_t bin = (key >> shift) & 255u;
+      if ((key & mask) == p0) atomicAdd(&h[0][bin], 1u);
+      if (q == 2 && (key & mask) == p1) atomicAdd(&h[1][bin], 1u);
+    }
+    __syncthreads();
+    for (int b = threadIdx.x; b < 256 * q; b += blockDim.x) {
+      const unsigned v = (&h[0][0])[b];
+      if (v) atomicAdd(&hist[(size_t)w * 512 + b], v);
+    }
+    if (threadIdx.x == 0 && nan_count) atomicAdd(&st[w].nan, nan_count);
+    __syncthreads();
+  }
+}
+
+// One warp per (segment, statistic): the bin that holds the wanted rank
+// becomes the next 8 bits of its prefix; the histogram is cleared.
+__global__ void select_pick_kernel(SelState* __restrict__ st, unsigned* __restrict__ hist,
+                                   int n_seg, int pass) {
+  const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  const long long w = gw >> 1;
+  const int qi = (int)(gw & 1);
+  if (w >= n_seg) return;
+  unsigned* h = hist + (size_t)w * 512 + qi * 256;
+  if (qi < st[w].q) {
+    unsigned c[8], tot = 0;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      c[j] = h[lane * 8 + j];
+      tot += c[j];
+    }
+    unsigned incl = tot;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned v = __shfl_up_sync(kFull, incl, o);
+      if (lane >= o) incl += v;
+    }
+    const unsigned excl = incl - tot;
+    const uint32_t r = st[w].rank[qi];
+    if (r >= excl && r < incl) {
+      unsigned acc = excl;
+      for (int j = 0; j < 8; ++j) {
+        if (r < acc + c[j]) {
+          const int shift = 24 - 8 * pass;
+          st[w].prefix[qi] |= (uint32_t)(lane * 8 + j) << shift;
+          st[w].rank[qi] = r - acc;
+          break;
+        }
+        acc += c[j];
+      }
+    }
+  }
+  __syncwarp();
+#pragma unroll
+  for (int j = 0; j < 8; ++j) h[lane * 8 + j] = 0;
+}
+
+// NumPy's median from the order statistics: NaN if any NaN, else the middle
+// value, or the float32 sum of the two middle values divided by 2.
+__global__ void select_finish_kernel(const SelState* __restrict__ st, int n_seg, int len,
+                                     float* __restrict__ out) {
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= n_seg) return;
+  const SelState s = st[w];
+  float v;
+  if (len == 0 || s.nan) {
+    v = __uint_as_float(0x7FC00000u);
+  } else if (s.q == 1) {
+    v = np_divide_count(__fadd_rn(0.0f, key_float(s.prefix[0])), 1);
+  } else {
+    const float sum = __fadd_rn(key_float(s.prefix[0]), key_float(s.prefix[1]));
+    v = np_divide_count(__fadd_rn(0.0f, sum), 2);
+  }
+  out[w] = v;
+}
+
+int np_median(const float* x, long long seg_stride, int len, int n_seg, int mode,
+              const float* centre, float* out, Scratch& sc, cudaStream_t st) {
+  SelState* state = nullptr;
+  unsigned* hist = nullptr;
+  BP_TRY(sc.get(&state, n_seg));
+  BP_TRY(sc.get(&hist, (size_t)n_seg * 512));
+  BP_CUDA(cudaMemsetAsync(hist, 0, (size_t)n_seg * 512 * sizeof(unsigned), st));
+  select_init_kernel<<<grid_for(n_seg, 256), 256, 0, st>>>(state, n_seg, len);
+  BP_LAUNCHED("select_init_kernel");
+  if (len > 0) {
+    const unsigned gx = grid_for(len, 256 * 16, 1024);
+    dim3 g(gx, (unsigned)std::min(n_seg, 65535));
+    for (int pass = 0; pass < 4; ++pass) {
+      select_hist_kernel<<<g, 256, 0, st>>>(x, seg_stride, len, mode, centre, n_seg, pass, state,
+                                            hist);
+      BP_LAUNCHED("select_hist_kernel");
+      select_pick_kernel<<<grid_for((long long)n_seg * 64, 256), 256, 0, st>>>(state, hist,
+                                                                               n_seg, pass);
+      BP_LAUNCHED("select_pick_kernel");
+    }
+  }
+  select_finish_kernel<<<grid_for(n_seg, 256), 256, 0, st>>>(state, n_seg, len, out);
+  BP_LAUNCHED("select_finish_kernel");
+  return BP_OK;
+}
+
+// ---- flag compaction (order preserving) -------------------------------------
+// rank = exclusive prefix sum of flags over n + 1 entries (flags[n] == 0), so
+// rank[n] is the number of flagged entries.
+int scan_flags(const int* flags, int* rank, int n, Scratch& sc, cudaStream_t st) {
+  size_t bytes = 0;
+  BP_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, bytes, flags, rank, n + 1, st));
+  void* tmp = nullptr;
+  BP_TRY(sc.get(reinterpret_cast<char**>(&tmp), bytes));
+  BP_CUDA(cub::DeviceScan::ExclusiveSum(tmp, bytes, flags, rank, n + 1, st));
+  return BP_OK;
+}
+
+// ---- threshold kernels ---------------------------------------------------------
+__global__ void zero_flags_kernel(const float* __restrict__ x, int n, int* __restrict__ flags) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i > n) return;
+  flags[i] = (i < n && x[i] == 0.0f) ? 1 : 0;
+}
+
+// Non-zero samples, in order, into nz.
+__global__ void gather_nonzero_kernel(const float* __restrict__ x, int n,
+                                      const int* __restrict__ zero_rank, float* __restrict__ nz) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float v = x[i];
+  if (v != 0.0f) nz[i - zero_rank[i]] = v;
+}
+
+// SplitMix64 output function (Steele, Lea & Flood, OOPSLA 2014).
+__device__ __forceinline__ uint64_t mix64(uint64_t z) {
+  z += 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+// Standard normal draws: Box-Muller on two counter-based uniforms.
+__global__ void normal_kernel(unsigned long long seed, int n, float* __restrict__ out) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint64_t a = mix64(seed ^ mix64(2ull * (uint64_t)i));
+  const uint64_t b = mix64(seed ^ mix64(2ull * (uint64_t)i + 1ull));
+  const float u1 = ((float)(a >> 40) + 0.5f) * 0x1p-24f;  // (0, 1)
+  const float u2 = (float)(b >> 40) * 0x1p-24f;           // [0, 1)
+  out[i] = sqrtf(-2.0f * logf(u1)) * cospif(2.0f * u2);
+}
+
+// Zeros replaced by noise * deviation + centre (NumPy float32 multiply, add).
+__global__ void fill_zeros_kernel(const float* __restrict__ x, int n,
+                                  const int* __restrict__ zero_rank,
+                                  const float* __restrict__ noise,
+                                  const float* __restrict__ centre0,
+                                  const float* __restrict__ dev0, float* __restrict__ out) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float v = x[i];
+  out[i] = v != 0.0f ? v : __fadd_rn(__fmul_rn(noise[zero_rank[i]], *dev0), *centre0);
+}
+
+// Default centre / deviation for the rms rule: deviation = sqrt(variance);
+// both NaN when there is no non-zero sample (NumPy's mean of nothing).
+__global__ void finish_stats_kernel(float* __restrict__ stats, int have) {
+  if (threadIdx.x != 0) return;
+  if (have) {
+    stats[1] = __fsqrt_rn(stats[1]);
+  } else {
+    stats[0] = stats[1] = __uint_as_float(0x7FC00000u);
+  }
+}
+
+// np.maximum on float32: NaN propagates, equal values give the second operand.
+__device__ __forceinline__ float np_maximum(float a, float b) {
+  return (a > b || isnan(a)) ? a : b;
+}
+
+// thr[w] = centre + num_dev * deviation (rms: deviation = sqrt(variance)).
+__global__ void window_threshold_kernel(const float* __restrict__ centre,
+                                        const float* __restrict__ spread, int n_win, int is_var,
+                                        float num_dev, float* __restrict__ thr) {
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= n_win) return;
+  const float dev = is_var ? __fsqrt_rn(spread[w]) : spread[w];
+  thr[w] = __fadd_rn(centre[w], __fmul_rn(num_dev, dev));
+}
+
+// neighbour = -1: out[i] = max(in[i-1], in[i]) for i >= 1 (in[0] kept);
+// neighbour = +1: out[i] = max(in[i], in[i+1]) for i < n-1 (in[n-1] kept).
+__global__ void neighbour_max_kernel(const float* __restrict__ in, int n_win, int neighbour,
+                                     float* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_win) return;
+  float v = in[i];
+  if (neighbour < 0 && i >= 1) v = np_maximum(in[i - 1], in[i]);
+  if (neighbour > 0 && i + 1 < n_win) v = np_maximum(in[i], in[i + 1]);
+  out[i] = v;
+}
+
+// Per-sample threshold: windows' values at (half + j) / shift for the middle
+// samples, the first / last middle value repeated at both ends.
+__global__ void spread_threshold_kernel(const float* __restrict__ thr, int n_win, int n,
+                                        int window, int half, int shift, float* __restrict__ out) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const long long n_mid = (long long)n - window;
+  long long j = i - half;
+  if (j < 0) j = 0;
+  if (j > n_mid - 1) j = n_mid - 1;
+  long long idx = (half + j) / shift;
+  if (idx > n_win - 1) idx = n_win - 1;
+  out[i] = thr[idx];
+}
+
+// ---- peak kernels ----------------------------------------------------------
+// Rising edges x[i-1] < x[i]: a peak at i when x[i+1] < x[i]; a plateau to
+// measure when x[i+1] == x[i].
+__global__ void local_max_kernel(const float* __restrict__ x, int n, int* __restrict__ flags,
+                                 int* __restrict__ plateau, int* __restrict__ n_plateau) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < 1 || i >= (long long)n - 1) return;
+  const float xi = x[i];
+  if (!(x[i - 1] < xi)) return;
+  const float nx = x[i + 1];
+  if (nx < xi) {
+    flags[i] = 1;
+  } else if (nx == xi) {
+    plateau[atomicAdd(n_plateau, 1)] = (int)i;
+  }
+}
+
+// One warp per plateau starting at i: its end j is the first index > i with
+// x[j] != x[i], capped at n - 1; a peak at (i + j - 1) / 2 when x[j] < x[i].
+__global__ void plateau_kernel(const float* __restrict__ x, int n, const int* __restrict__ plateau,
+                               const int* __restrict__ n_plateau, int* __restrict__ flags) {
+  const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (gw >= *n_plateau) return;
+  const int i = plateau[gw];
+  const float xi = x[i];
+  for (long long base = (long long)i + 1;; base += 32) {
+    const long long j = base + lane;
+    const bool stop = j >= (long long)n - 1 || x[j] != xi;
+    const unsigned b = __ballot_sync(kFull, stop);
+    if (b) {
+      long long e = base + __ffs(b) - 1;
+      if (e > n - 1) e = n - 1;
+      if (lane == 0 && x[e] < xi) flags[(i + e - 1) / 2] = 1;
+      return;
+    }
+  }
+}
+
+__global__ void scatter_flagged_kernel(const int* __restrict__ flags, const int* __restrict__ rank,
+                                       int n, int* __restrict__ out) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  if (flags[i]) out[rank[i]] = (int)i;
+}
+
+__global__ void gather_heights_kernel(const float* __restrict__ x, const int* __restrict__ pos,
+                                      int m, float* __restrict__ val, int* __restrict__ state,
+                                      int* __restrict__ undecided) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= m) return;
+  val[j] = x[pos[j]];
+  state[j] = 0;
+  undecided[j] = j;
+}
+
+enum : int { kUndecided = 0, kKept = 1, kDropped = 2 };
+
+// Peak k goes before peak j in SciPy's order (decreasing height; the later
+// sample first among equal heights, as a stable ascending sort read backwards).
+__device__ __forceinline__ bool before(const float* val, int k, int j) {
+  return val[k] > val[j] || (val[k] == val[j] && k > j);
+}
+
+// Round step 1, one warp per undecided peak: kept when no undecided peak
+// within the distance goes before it.
+__global__ void distance_keep_kernel(const int* __restrict__ pos, const float* __restrict__ val,
+                                     const int* __restrict__ state, int m, long long dist,
+                                     const int* __restrict__ undecided, int n_undecided,
+                                     int* __restrict__ kept, int* __restrict__ n_kept) {
+  const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (gw >= n_undecided) return;
+  const int j = undecided[gw];
+  const long long pj = pos[j];
+  bool blocked = false;
+  for (long long base = (long long)j - 1; base >= 0; base -= 32) {
+    const long long k = base - lane;
+    const bool in = k >= 0 && pj - pos[k] < dist;
+    const bool blk = in && state[k] == kUndecided && before(val, (int)k, j);
+    if (__any_sync(kFull, blk)) {
+      blocked = true;
+      break;
+    }
+    if (__any_sync(kFull, !in)) break;
+  }
+  if (!blocked) {
+    for (long long base = (long long)j + 1; base < m; base += 32) {
+      const long long k = base + lane;
+      const bool in = k < m && pos[k] - pj < dist;
+      const bool blk = in && state[k] == kUndecided && before(val, (int)k, j);
+      if (__any_sync(kFull, blk)) {
+        blocked = true;
+        break;
+      }
+      if (__any_sync(kFull, !in)) break;
+    }
+  }
+  if (!blocked && lane == 0) kept[atomicAdd(n_kept, 1)] = j;
+}
+
+// Round step 2, one warp per newly kept peak: mark it kept and drop every
+// undecided peak within the distance.
+__global__ void distance_drop_kernel(const int* __restrict__ pos, int* __restrict__ state, int m,
+                                     long long dist, const int* __restrict__ kept,
+                                     const int* __restrict__ n_kept) {
+  const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (gw >= *n_kept) return;
+  const int j = kept[gw];
+  const long long pj = pos[j];
+  if (lane == 0) state[j] = kKept;
+  for (long long base = (long long)j - 1; base >= 0; base -= 32) {
+    const long long k = base - lane;
+    const bool in = k >= 0 && pj - pos[k] < dist;
+    if (in && state[k] == kUndecided) state[k] = kDropped;
+    if (__any_sync(kFull, !in)) break;
+  }
+  for (long long base = (long long)j + 1; base < m; base += 32) {
+    const long long k = base + lane;
+    const bool in = k < m && pos[k] - pj < dist;
+    if (in && state[k] == kUndecided) state[k] = kDropped;
+    if (__any_sync(kFull, !in)) break;
+  }
+}
+
+// Round step 3: the still undecided peaks form the next work list.
+__global__ void distance_next_kernel(const int* __restrict__ state,
+                                     const int* __restrict__ undecided, int n_undecided,
+                                     int* __restrict__ next, int* __restrict__ n_next) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_undecided) return;
+  const int j = undecided[i];
+  if (state[j] == kUndecided) next[atomicAdd(n_next, 1)] = j;
+}
+
+__global__ void kept_flags_kernel(const int* __restrict__ state, int m, int* __restrict__ flags) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j > m) return;
+  flags[j] = (j < m && state[j] == kKept) ? 1 : 0;
+}
+
+__global__ void scatter_peaks_kernel(const int* __restrict__ flags, const int* __restrict__ rank,
+                                     const int* __restrict__ pos, int m, int* __restrict__ out) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= m) return;
+  if (flags[j]) out[rank[j]] = pos[j];
+}
+
+__global__ void above_flags_kernel(const float* __restrict__ x, const float* __restrict__ thr,
+                                   const int* __restrict__ peaks, int m, int* __restrict__ flags) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j > m) return;
+  flags[j] = (j < m && x[peaks[j]] > thr[peaks[j]]) ? 1 : 0;
+}
+
+__global__ void scatter_detections_kernel(const int* __restrict__ flags,
+                                          const int* __restrict__ rank,
+                                          const int* __restrict__ peaks, int m,
+                                          const float* __restrict__ x,
+                                          const int32_t* __restrict__ argmax,
+                                          int32_t* __restrict__ out_peaks,
+                                          float* __restrict__ out_heights,
+                                          int32_t* __restrict__ out_sources) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= m || !flags[j]) return;
+  const int r = rank[j], p = peaks[j];
+  out_peaks[r] = p;
+  if (out_heights) out_heights[r] = x[p];
+  if (argmax && out_sources) out_sources[r] = argmax[p];
+}
+
+// ---- host drivers -------------------------------------------------------------
+// Peaks of x into d_peaks (device, ascending); their number into *m_out.
+int find_peaks_impl(const float* x, int n, double distance, int32_t* d_peaks, int* m_out,
+                    Scratch& sc, cudaStream_t st) {
+  *m_out = 0;
+  if (n < 3) return BP_OK;
+  int *flags = nullptr, *rank = nullptr, *plateau = nullptr, *counters = nullptr;
+  BP_TRY(sc.get(&flags, (size_t)n + 1));
+  BP_TRY(sc.get(&rank, (size_t)n + 1));
+  BP_TRY(sc.get(&plateau, n));
+  BP_TRY(sc.get(&counters, 4));
+  BP_CUDA(cudaMemsetAsync(flags, 0, ((size_t)n + 1) * sizeof(int), st));
+  BP_CUDA(cudaMemsetAsync(counters, 0, 4 * sizeof(int), st));
+  local_max_kernel<<<grid_for(n, 256), 256, 0, st>>>(x, n, flags, plateau, counters);
+  BP_LAUNCHED("local_max_kernel");
+  int n_plateau = 0;
+  BP_TRY(read_back(&n_plateau, counters, st));
+  if (n_plateau > 0) {
+    plateau_kernel<<<grid_for((long long)n_plateau * 32, 256), 256, 0, st>>>(x, n, plateau,
+                                                                             counters, flags);
+    BP_LAUNCHED("plateau_kernel");
+  }
+  BP_TRY(scan_flags(flags, rank, n, sc, st));
+  int m = 0;
+  BP_TRY(read_back(&m, rank + n, st));
+  const bool by_distance = distance > 0.0 && m > 1;
+  int* pos = by_distance ? nullptr : d_peaks;
+  if (by_distance) BP_TRY(sc.get(&pos, m));
+  scatter_flagged_kernel<<<grid_for(n, 256), 256, 0, st>>>(flags, rank, n, pos);
+  BP_LAUNCHED("scatter_flagged_kernel");
+  if (!by_distance) {
+    *m_out = m;
+    return BP_OK;
+  }
+  // greedy distance rule, in rounds
+  const double dc = std::ceil(distance);
+  const long long dist = dc > (double)n ? (long long)n + 1 : (long long)dc;
+  float* val = nullptr;
+  int *state = nullptr, *und = nullptr, *und2 = nullptr, *kept = nullptr;
+  BP_TRY(sc.get(&val, m));
+  BP_TRY(sc.get(&state, (size_t)m + 1));
+  BP_TRY(sc.get(&und, m));
+  BP_TRY(sc.get(&und2, m));
+  BP_TRY(sc.get(&kept, m));
+  gather_heights_kernel<<<grid_for(m, 256), 256, 0, st>>>(x, pos, m, val, state, und);
+  BP_LAUNCHED("gather_heights_kernel");
+  int u = m;
+  for (int round = 0; u > 0; ++round) {
+    if (round > m) return fail(BP_ERR_KERNEL, "distance rule did not converge");
+    BP_CUDA(cudaMemsetAsync(counters + 1, 0, 2 * sizeof(int), st));
+    const unsigned gw = grid_for((long long)u * 32, 256);
+    distance_keep_kernel<<<gw, 256, 0, st>>>(pos, val, state, m, dist, und, u, kept,
+                                             counters + 1);
+    BP_LAUNCHED("distance_keep_kernel");
+    distance_drop_kernel<<<gw, 256, 0, st>>>(pos, state, m, dist, kept, counters + 1);
+    BP_LAUNCHED("distance_drop_kernel");
+    distance_next_kernel<<<grid_for(u, 256), 256, 0, st>>>(state, und, u, und2, counters + 2);
+    BP_LAUNCHED("distance_next_kernel");
+    BP_TRY(read_back(&u, counters + 2, st));
+    std::swap(und, und2);
+  }
+  kept_flags_kernel<<<grid_for((long long)m + 1, 256), 256, 0, st>>>(state, m, flags);
+  BP_LAUNCHED("kept_flags_kernel");
+  BP_TRY(scan_flags(flags, rank, m, sc, st));
+  int k = 0;
+  BP_TRY(read_back(&k, rank + m, st));
+  scatter_peaks_kernel<<<grid_for(m, 256), 256, 0, st>>>(flags, rank, pos, m, d_peaks);
+  BP_LAUNCHED("scatter_peaks_kernel");
+  *m_out = k;
+  return BP_OK;
+}
+
+int check_series(const void* p, size_t n, const char* what) {
+  if (!p && n) return fail(BP_ERR_INVALID_ARGUMENT, "%s is NULL", what);
+  if (n > (size_t)INT_MAX - 1) return fail(BP_ERR_UNSUPPORTED, "%s longer than 2^31 - 2", what);
+  return BP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+float bp_pairwise_sum_f32(const float* x, size_t n) {
+  if (n == 0 || !x || n > (size_t)INT_MAX) return 0.0f;
+  const PwTree t = pw_tree((int)n);
+  std::vector<float> v(t.n_nodes);
+  for (const int4& lf : t.leaves) {
+    const float* base = x + lf.y;
+    v[lf.x] = pw_leaf([&](int i) { return base[i]; }, lf.z);
+  }
+  for (const int4& nd : t.inner) v[nd.x] = v[nd.y] + v[nd.z];
+  return 0.0f + v[t.root];
+}
+
+int bp_threshold_dev(const float* d_series, size_t n_samples, size_t sliding_window,
+                     double overlap, int kind, float num_dev, const float* d_white_noise,
+                     size_t n_white_noise, unsigned long long seed, float* d_threshold,
+                     void* stream) {
+  BP_TRY(check_series(d_series, n_samples, "series"));
+  if (!d_threshold) return fail(BP_ERR_INVALID_ARGUMENT, "threshold output is NULL");
+  if (kind != BP_THRESHOLD_RMS && kind != BP_THRESHOLD_MAD)
+    return fail(BP_ERR_INVALID_ARGUMENT, "threshold kind must be rms (0) or mad (1)");
+  if (sliding_window < 1 || n_samples <= sliding_window)
+    return fail(BP_ERR_INVALID_ARGUMENT,
+                "the series (%zu samples) must be longer than the sliding window (%zu)",
+                n_samples, sliding_window);
+  const double step = (1.0 - overlap) * (double)sliding_window;
+  if (!(step >= 1.0) || step > (double)INT_MAX)
+    return fail(BP_ERR_INVALID_ARGUMENT, "(1 - overlap) * sliding_window must be in [1, 2^31)");
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  const int n = (int)n_samples, W = (int)sliding_window, half = W / 2;
+  const int shift = (int)step;  // int() truncation, as in the notebook
+  const int n_win = (n - W) / shift + 1;
+  Scratch sc(st);
+  int *zflags = nullptr, *zrank = nullptr;
+  float *nz = nullptr, *filled = nullptr, *stats0 = nullptr;
+  BP_TRY(sc.get(&zflags, (size_t)n + 1));
+  BP_TRY(sc.get(&zrank, (size_t)n + 1));
+  BP_TRY(sc.get(&nz, n));
+  BP_TRY(sc.get(&filled, n));
+  BP_TRY(sc.get(&stats0, 2));  // default centre, deviation
+  zero_flags_kernel<<<grid_for((long long)n + 1, 256), 256, 0, st>>>(d_series, n, zflags);
+  BP_LAUNCHED("zero_flags_kernel");
+  BP_TRY(scan_flags(zflags, zrank, n, sc, st));
+  int n_zeros = 0;
+  BP_TRY(read_back(&n_zeros, zrank + n, st));
+  if (d_white_noise && n_white_noise < (size_t)n_zeros)
+    return fail(BP_ERR_INVALID_ARGUMENT, "white noise holds %zu values for %d zero samples",
+                n_white_noise, n_zeros);
+  const int m = n - n_zeros;
+  gather_nonzero_kernel<<<grid_for(n, 256), 256, 0, st>>>(d_series, n, zrank, nz);
+  BP_LAUNCHED("gather_nonzero_kernel");
+  // centre and deviation of the non-zero samples (NaN when there are none)
+  if (kind == BP_THRESHOLD_RMS) {
+    if (m > 0) {
+      BP_TRY(pw_mean(nz, 0, m, 1, 0, nullptr, stats0, sc, st));
+      BP_TRY(pw_mean(nz, 0, m, 1, 1, stats0, stats0 + 1, sc, st));
+    }
+    finish_stats_kernel<<<1, 32, 0, st>>>(stats0, m > 0 ? 1 : 0);
+    BP_LAUNCHED("finish_stats_kernel");
+  } else {
+    BP_TRY(np_median(nz, 0, m, 1, 0, nullptr, stats0, sc, st));
+    BP_TRY(np_median(nz, 0, m, 1, 1, stats0, stats0 + 1, sc, st));
+  }
+  const float* noise = d_white_noise;
+  if (n_zeros > 0 && !noise) {
+    float* gen = nullptr;
+    BP_TRY(sc.get(&gen, n_zeros));
+    normal_kernel<<<grid_for(n_zeros, 256), 256, 0, st>>>(seed, n_zeros, gen);
+    BP_LAUNCHED("normal_kernel");
+    noise = gen;
+  }
+  fill_zeros_kernel<<<grid_for(n, 256), 256, 0, st>>>(d_series, n, zrank, noise, stats0,
+                                                       stats0 + 1, filled);
+  BP_LAUNCHED("fill_zeros_kernel");
+  // per-window centre and spread
+  float *centre = nullptr, *spread = nullptr, *thr = nullptr, *thr2 = nullptr;
+  BP_TRY(sc.get(&centre, n_win));
+  BP_TRY(sc.get(&spread, n_win));
+  BP_TRY(sc.get(&thr, n_win));
+  BP_TRY(sc.get(&thr2, n_win));
+  if (kind == BP_THRESHOLD_RMS) {
+    BP_TRY(pw_mean(filled, shift, W, n_win, 0, nullptr, centre, sc, st));
+    BP_TRY(pw_mean(filled, shift, W, n_win, 1, centre, spread, sc, st));
+  } else {
+    BP_TRY(np_median(filled, shift, W, n_win, 0, nullptr, centre, sc, st));
+    BP_TRY(np_median(filled, shift, W, n_win, 1, centre, spread, sc, st));
+  }
+  const unsigned gwin = grid_for(n_win, 256);
+  window_threshold_kernel<<<gwin, 256, 0, st>>>(centre, spread, n_win,
+                                                kind == BP_THRESHOLD_RMS ? 1 : 0, num_dev, thr);
+  BP_LAUNCHED("window_threshold_kernel");
+  neighbour_max_kernel<<<gwin, 256, 0, st>>>(thr, n_win, -1, thr2);
+  BP_LAUNCHED("neighbour_max_kernel");
+  neighbour_max_kernel<<<gwin, 256, 0, st>>>(thr2, n_win, +1, thr);
+  BP_LAUNCHED("neighbour_max_kernel");
+  spread_threshold_kernel<<<grid_for(n, 256), 256, 0, st>>>(thr, n_win, n, W, half, shift,
+                                                            d_threshold);
+  BP_LAUNCHED("spread_threshold_kernel");
+  return BP_OK;
+}
+
+int bp_find_peaks_dev(const float* d_x, size_t n_samples, double distance, int32_t* d_peaks,
+                      size_t capacity, size_t* n_peaks, void* stream) {
+  BP_TRY(check_series(d_x, n_samples, "series"));
+  if (!n_peaks) return fail(BP_ERR_INVALID_ARGUMENT, "n_peaks is NULL");
+  *n_peaks = 0;
+  if (distance > 0.0 && distance < 1.0)
+    return fail(BP_ERR_INVALID_ARGUMENT, "distance must be greater or equal to 1");
+  if (capacity < n_samples / 2 || (!d_peaks && n_samples >= 3))
+    return fail(BP_ERR_INVALID_ARGUMENT, "peak capacity must be at least n_samples / 2");
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  Scratch sc(st);
+  int m = 0;
+  BP_TRY(find_peaks_impl(d_x, (int)n_samples, distance, d_peaks, &m, sc, st));
+  *n_peaks = (size_t)m;
+  return BP_OK;
+}
+
+int bp_detect_dev(const float* d_beam_max, const int32_t* d_argmax, const float* d_threshold,
+                  size_t n_samples, double distance, int32_t* d_peaks, float* d_heights,
+                  int32_t* d_sources, size_t capacity, size_t* n_detections, void* stream) {
+  BP_TRY(check_series(d_beam_max, n_samples, "beam_max"));
+  BP_TRY(check_series(d_threshold, n_samples, "threshold"));
+  if (!n_detections) return fail(BP_ERR_INVALID_ARGUMENT, "n_detections is NULL");
+  *n_detections = 0;
+  if (distance > 0.0 && distance < 1.0)
+    return fail(BP_ERR_INVALID_ARGUMENT, "distance must be greater or equal to 1");
+  if (capacity < n_samples / 2 || (!d_peaks && n_samples >= 3))
+    return fail(BP_ERR_INVALID_ARGUMENT, "detection capacity must be at least n_samples / 2");
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  Scratch sc(st);
+  const int n = (int)n_samples;
+  int* peaks = nullptr;
+  BP_TRY(sc.get(&peaks, n / 2 + 1));
+  int m = 0;
+  BP_TRY(find_peaks_impl(d_beam_max, n, distance, peaks, &m, sc, st));
+  if (m == 0) return BP_OK;
+  int *flags = nullptr, *rank = nullptr;
+  BP_TRY(sc.get(&flags, (size_t)m + 1));
+  BP_TRY(sc.get(&rank, (size_t)m + 1));
+  above_flags_kernel<<<grid_for((long long)m + 1, 256), 256, 0, st>>>(d_beam_max, d_threshold,
+                                                                      peaks, m, flags);
+  BP_LAUNCHED("above_flags_kernel");
+  BP_TRY(scan_flags(flags, rank, m, sc, st));
+  int k = 0;
+  BP_TRY(read_back(&k, rank + m, st));
+  scatter_detections_kernel<<<grid_for(m, 256), 256, 0, st>>>(
+      flags, rank, peaks, m, d_beam_max, d_argmax, d_peaks, d_heights, d_sources);
+  BP_LAUNCHED("scatter_detections_kernel");
+  BP_CUDA(cudaStreamSynchronize(st));
+  *n_detections = (size_t)k;
+  return BP_OK;
+}
+
+}  // extern "C"

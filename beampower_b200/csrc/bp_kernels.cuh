@@ -772,9 +772,10 @@ beam_batch_kernel(const LaunchArgs a) {
   }
 }
 
-// Everything below holds non-template kernels (one definition per program), so
-// the files that only instantiate the staged kernel leave it out.
-#ifndef BP_STAGED_KERNELS_ONLY
+// Everything below holds non-template kernels (one definition per program):
+// translation units other than bp_capi.cu define BP_TEMPLATE_KERNELS_ONLY and
+// leave it out.
+#ifndef BP_TEMPLATE_KERNELS_ONLY
 
 // Decode every record's keys of a batch into its outputs.
 __global__ void batch_decode_kernel(const RecordView* __restrict__ recs) {
@@ -1186,6 +1187,6 @@ __global__ void prestack_h16_kernel(const float* __restrict__ F, const float* __
   }
 }
 
-#endif  // BP_STAGED_KERNELS_ONLY
+#endif  // BP_TEMPLATE_KERNELS_ONLY
 
 }  // namespace bp

@@ -4,7 +4,7 @@
 
 #include <algorithm>
 
-#define BP_STAGED_KERNELS_ONLY
+#define BP_TEMPLATE_KERNELS_ONLY
 #include "bp_host.h"
 
 namespace bp_host {

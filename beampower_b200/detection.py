@@ -1,0 +1,161 @@
+"""Detection on the beam series, on the GPU.
+
+The reference tutorial turns ``beam_max`` into detections in two notebook
+cells: a time-dependent threshold (notebooks/3_beampower.ipynb:497-579,
+``time_dependent_threshold``) and ``scipy.signal.find_peaks(beam_max,
+distance=...)`` followed by the strict threshold test
+(notebooks/3_beampower.ipynb:618-626).  The functions here run both on the
+device and give identical results: float32 arithmetic in NumPy's order for
+the threshold, SciPy's rules for the peaks.
+
+Inputs are numpy arrays or torch tensors; CUDA tensors stay on their device.
+Outputs follow the input: numpy in, numpy out; tensor in, tensor out.
+"""
+from __future__ import annotations
+
+import ctypes as ct
+from dataclasses import dataclass
+
+import numpy as np
+
+from .core import check, load_library
+
+try:
+    import torch
+except ImportError:  # pragma: no cover
+    torch = None
+
+THRESHOLD_KINDS = {"rms": 0, "mad": 1}
+
+
+def _as_device(x, dtype):
+    from .tables import _dev_tensor
+    if torch is None:
+        raise RuntimeError("torch is required for the detection functions")
+    dev = x.device if isinstance(x, torch.Tensor) and x.is_cuda else torch.device(
+        "cuda", torch.cuda.current_device())
+    return _dev_tensor(x, dtype, dev)
+
+
+def _is_tensor(x):
+    return torch is not None and isinstance(x, torch.Tensor)
+
+
+def _out(t, like):
+    return t if _is_tensor(like) else t.cpu().numpy()
+
+
+def time_dependent_threshold(time_series, sliding_window, overlap=0.66, threshold_type="rms",
+                             num_dev=8.0, white_noise=None, seed=0):
+    """Per-sample detection threshold of a beam series (float32).
+
+    Same arguments and result as the tutorial's ``time_dependent_threshold``
+    (notebooks/3_beampower.ipynb:497): zero samples are replaced by white
+    noise scaled by the non-zero samples' centre and deviation; every
+    ``int((1 - overlap) * sliding_window)`` samples a window of
+    ``sliding_window`` samples gives centre + num_dev * deviation (mean and
+    standard deviation for 'rms', median and median absolute deviation for
+    'mad'); the window values are max-filtered with their neighbours and
+    spread back to every sample.
+
+    white_noise: the standard normal draws for the zero samples, in sample
+    order (the tutorial draws ``np.random.normal(size=n_zeros)``); when None
+    they come from this library's generator seeded by ``seed``.
+    """
+    lib = load_library("gpu")
+    kind = THRESHOLD_KINDS.get(str(threshold_type).lower())
+    if kind is None:
+        raise ValueError("threshold_type must be 'rms' or 'mad'")
+    x = _as_device(time_series, torch.float32)
+    if x.ndim != 1:
+        raise ValueError("time_series must be one-dimensional")
+    n = int(x.shape[0])
+    out = torch.empty(n, dtype=torch.float32, device=x.device)
+    noise_ptr, n_noise = None, 0
+    if white_noise is not None:
+        noise = _as_device(white_noise, torch.float32).reshape(-1)
+        noise_ptr, n_noise = noise.data_ptr(), int(noise.shape[0])
+    from .tables import _stream_ptr
+    with torch.cuda.device(x.device):
+        rc = lib.bp_threshold_dev(x.data_ptr(), n, int(sliding_window), float(overlap), kind,
+                                  float(num_dev), noise_ptr, n_noise, int(seed) & (2**64 - 1),
+                                  out.data_ptr(), _stream_ptr())
+    if rc == 1:
+        raise ValueError(lib.bp_last_error().decode())
+    check(rc)
+    return _out(out, time_series)
+
+
+def find_peaks(x, distance=None):
+    """``(peaks, {})`` as ``scipy.signal.find_peaks(x, distance=distance)``.
+
+    Peaks are the local maxima of x (a flat plateau counts at its midpoint
+    when both its neighbours are lower); with ``distance``, peaks are taken
+    in decreasing height and every peak closer than ``ceil(distance)``
+    samples to a taken one is dropped.  Equal heights: the later sample
+    first (SciPy leaves that order to NumPy's unstable sort).
+    """
+    lib = load_library("gpu")
+    d = _as_device(x, torch.float32)
+    if d.ndim != 1:
+        raise ValueError("x must be one-dimensional")
+    if distance is not None and distance < 1:
+        raise ValueError("`distance` must be greater or equal to 1")
+    n = int(d.shape[0])
+    cap = max(n // 2, 1)
+    peaks = torch.empty(cap, dtype=torch.int32, device=d.device)
+    count = ct.c_size_t(0)
+    from .tables import _stream_ptr
+    with torch.cuda.device(d.device):
+        check(lib.bp_find_peaks_dev(d.data_ptr(), n, 0.0 if distance is None else float(distance),
+                                    peaks.data_ptr(), cap, ct.byref(count), _stream_ptr()))
+    p = peaks[:count.value].to(torch.int64)
+    return _out(p, x), {}
+
+
+@dataclass
+class Detections:
+    """Detected events: sample indexes, beam heights, winning sources
+    (None without ``beam_argmax``) and the threshold used."""
+
+    peaks: object
+    heights: object
+    sources: object
+    threshold: object
+
+
+def detect(beam_max, beam_argmax=None, threshold=None, distance=None, **threshold_kwargs):
+    """Detections of the tutorial (notebooks/3_beampower.ipynb:618-626): the
+    peaks of ``beam_max`` at least ``distance`` samples apart whose height is
+    strictly above ``threshold``.  Without ``threshold``, it is computed by
+    ``time_dependent_threshold(beam_max, **threshold_kwargs)``."""
+    lib = load_library("gpu")
+    bm = _as_device(beam_max, torch.float32)
+    if threshold is None:
+        thr = _as_device(time_dependent_threshold(bm, **threshold_kwargs), torch.float32)
+    else:
+        thr = _as_device(threshold, torch.float32)
+    if bm.ndim != 1 or thr.shape != bm.shape:
+        raise ValueError("beam_max and threshold must be one-dimensional and of one length")
+    if distance is not None and distance < 1:
+        raise ValueError("`distance` must be greater or equal to 1")
+    am = None if beam_argmax is None else _as_device(beam_argmax, torch.int32)
+    n = int(bm.shape[0])
+    cap = max(n // 2, 1)
+    peaks = torch.empty(cap, dtype=torch.int32, device=bm.device)
+    heights = torch.empty(cap, dtype=torch.float32, device=bm.device)
+    sources = torch.empty(cap, dtype=torch.int32, device=bm.device) if am is not None else None
+    count = ct.c_size_t(0)
+    from .tables import _stream_ptr
+    with torch.cuda.device(bm.device):
+        check(lib.bp_detect_dev(bm.data_ptr(), None if am is None else am.data_ptr(),
+                                thr.data_ptr(), n, 0.0 if distance is None else float(distance),
+                                peaks.data_ptr(), heights.data_ptr(),
+                                None if sources is None else sources.data_ptr(), cap,
+                                ct.byref(count), _stream_ptr()))
+    k = count.value
+    return Detections(peaks=_out(peaks[:k].to(torch.int64), beam_max),
+                      heights=_out(heights[:k], beam_max),
+                      sources=None if sources is None else _out(sources[:k].to(torch.int64),
+                                                                beam_max),
+                      threshold=_out(thr, beam_max) if threshold is None else threshold)

@@ -2,7 +2,8 @@
  * beampower_b200 -- C-ABI of the sm_100a beamforming library
  * (beampower_b200/lib/libbeampower_b200.so).
  *
- * Two groups of entry points:
+ * Three groups of entry points (the third, detection on the beam series,
+ * is described at its section below):
  *
  * 1. Drop-ins for the reference's GPU library.  Same symbol names, argument
  *    order and meaning as beampower/src/beamform_gpu.h:1-2, bound by
@@ -285,6 +286,57 @@ BP_API int bp_beamform_differential_dev(const float *d_traces, size_t n_samples,
                                         const float *d_weights_sources, size_t n_sources,
                                         size_t n_stations, size_t n_phases, float *d_beam,
                                         void *stream);
+
+/* ======================================================================= */
+/* 3. Detection on the beam series (the step after beamform_max)           */
+/* ======================================================================= */
+/* The reference tutorial turns beam_max into detections in two notebook
+ * cells; these entry points restate them on the device with identical
+ * results (float32 arithmetic in NumPy's own order, SciPy's peak rules).
+ * Each allocates its scratch with cudaMallocAsync on `stream` and
+ * synchronises `stream` (it reads counts back), so none of them can be
+ * captured in a CUDA graph. */
+
+#define BP_THRESHOLD_RMS 0 /* window mean + num_dev * standard deviation */
+#define BP_THRESHOLD_MAD 1 /* window median + num_dev * median |x - median| */
+
+/* Time-dependent detection threshold, one value per sample
+ * (notebooks/3_beampower.ipynb:497-579, time_dependent_threshold).  Zero
+ * samples are first replaced by noise * deviation + centre of the non-zero
+ * samples: d_white_noise holds the standard normal draws in sample order
+ * (n_white_noise >= number of zeros); NULL draws them from this library's
+ * own generator seeded by `seed` (the notebook draws them from NumPy's global
+ * generator).  Windows of sliding_window samples start every
+ * int((1 - overlap) * sliding_window) samples.  Rejects n_samples <=
+ * sliding_window and a window step below 1 (the notebook raises there). */
+BP_API int bp_threshold_dev(const float *d_series, size_t n_samples, size_t sliding_window,
+                            double overlap, int kind, float num_dev,
+                            const float *d_white_noise, size_t n_white_noise,
+                            unsigned long long seed, float *d_threshold, void *stream);
+
+/* Peak sample indexes in increasing order, as
+ * scipy.signal.find_peaks(x, distance=distance)[0] (called at
+ * notebooks/3_beampower.ipynb:621): local maxima, flat plateaus by their
+ * midpoint, then, when distance > 0, the greedy rule that keeps peaks in
+ * decreasing height and drops every peak closer than ceil(distance) samples
+ * to a kept one (equal heights: the later sample first).  distance <= 0
+ * means no distance rule; 0 < distance < 1 is rejected as SciPy does.
+ * capacity must be at least n_samples / 2. */
+BP_API int bp_find_peaks_dev(const float *d_x, size_t n_samples, double distance,
+                             int32_t *d_peaks, size_t capacity, size_t *n_peaks, void *stream);
+
+/* Detections (notebooks/3_beampower.ipynb:618-626): the peaks of d_beam_max
+ * as above whose height is strictly above d_threshold, with their heights
+ * and, when d_argmax is not NULL, the winning source of each. */
+BP_API int bp_detect_dev(const float *d_beam_max, const int32_t *d_argmax,
+                         const float *d_threshold, size_t n_samples, double distance,
+                         int32_t *d_peaks, float *d_heights, int32_t *d_sources,
+                         size_t capacity, size_t *n_detections, void *stream);
+
+/* Host function: NumPy's float32 pairwise sum of x[0..n) (the summation
+ * order the threshold kernels reproduce), for checking that order without a
+ * GPU.  No reference counterpart. */
+BP_API float bp_pairwise_sum_f32(const float *x, size_t n);
 
 /* ---- staged-kernel configurations (autotuning) -------------------------- */
 /* The staged kernel exists in several shapes (sources per thread, samples per
