@@ -30,6 +30,7 @@ LINK_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-shared",
     "-cudart", "static",
+    "-lcufft",
 ]
 
 
@@ -95,7 +96,11 @@ def build(force: bool = False, verbose: bool = False, extra=(), jobs=None) -> st
     if failed:
         raise subprocess.CalledProcessError(1, "nvcc")
     tmp = LIB + ".tmp"
-    cmd = [nvcc(), *cc, *LINK_FLAGS, *(obj for _s, obj, _r in results), "-o", tmp]
+    # cuFFT (envelope features) is found through the toolkit's lib64 at run time
+    cuda_lib = os.path.join(os.path.dirname(os.path.dirname(os.path.realpath(
+        nvcc() if os.path.sep in nvcc() else "/usr/local/cuda/bin/nvcc"))), "lib64")
+    cmd = [nvcc(), *cc, *LINK_FLAGS, *(obj for _s, obj, _r in results),
+           "-Xlinker", "-rpath=" + cuda_lib, "-o", tmp]
     if verbose:
         print(" ".join(cmd), flush=True)
     subprocess.run(cmd, check=True)

@@ -113,6 +113,28 @@ class TravelTimeTable:
                                        _stream_ptr(stream)))
         return Traces(buf, scales, st, T, lpad, pitch)
 
+    def traces_from_waveforms(self, waveforms, weights_phases, storage="fp32", clip_max=1e5,
+                              stream=None):
+        """Raw (S, C, T) waveforms to this table's trace layout in one device
+        call: the tutorial's envelope feature of every (station, channel)
+        (notebooks/3_beampower.ipynb:74-103) and then the prestack."""
+        X = _dev_tensor(waveforms, torch.float32, self.device)
+        A = _dev_tensor(weights_phases, torch.float32, self.device)
+        S, C, T = map(int, X.shape)
+        if S != self.n_stations or A.shape != (S, C, self.n_phases):
+            raise ValueError("waveforms / weights_phases do not match the table")
+        st = STORAGE[storage]
+        lpad, pitch = self.layout(T)
+        elem = torch.float32 if st == 0 else (torch.bfloat16 if st == 1 else torch.float16)
+        rows = S * self.n_phases * (1 if st == 0 else 2)
+        buf = torch.empty((rows, pitch), dtype=elem, device=self.device)
+        scales = torch.ones(S, dtype=torch.float32, device=self.device)
+        check(self.lib.bp_prestack_envelope_dev(X.data_ptr(), A.data_ptr(), T, S, C,
+                                                self.n_phases, float(clip_max), st, lpad, pitch,
+                                                buf.data_ptr(), scales.data_ptr(),
+                                                _stream_ptr(stream)))
+        return Traces(buf, scales, st, T, lpad, pitch)
+
     def traces_from_prestacked(self, prestacked, stream=None):
         """(S, T, P) prestacked float32 traces -> this table's layout."""
         U = _dev_tensor(prestacked, torch.float32, self.device)

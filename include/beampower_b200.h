@@ -2,8 +2,8 @@
  * beampower_b200 -- C-ABI of the sm_100a beamforming library
  * (beampower_b200/lib/libbeampower_b200.so).
  *
- * Three groups of entry points (the third, detection on the beam series,
- * is described at its section below):
+ * Four groups of entry points; groups 3 (detection on the beam series) and
+ * 4 (waveform features) are described at their sections below:
  *
  * 1. Drop-ins for the reference's GPU library.  Same symbol names, argument
  *    order and meaning as beampower/src/beamform_gpu.h:1-2, bound by
@@ -332,6 +332,33 @@ BP_API int bp_detect_dev(const float *d_beam_max, const int32_t *d_argmax,
                          const float *d_threshold, size_t n_samples, double distance,
                          int32_t *d_peaks, float *d_heights, int32_t *d_sources,
                          size_t capacity, size_t *n_detections, void *stream);
+
+/* ======================================================================= */
+/* 4. Waveform features (the step before the prestack)                      */
+/* ======================================================================= */
+/* The reference tutorial's envelope transform (notebooks/3_beampower.ipynb:
+ * 74-103, `envelope`, applied to every trace at :145-147): the modulus of the
+ * analytic signal (scipy.signal.hilbert), minus its median, divided by its
+ * median absolute deviation (1 when that is 0), clipped above at clip_max
+ * (1e5 in the tutorial).  The FFTs run in cuFFT (float32), so results match
+ * the tutorial's float32 SciPy FFTs to rounding, not bit for bit.  Allocates
+ * scratch with cudaMallocAsync on `stream`; cuFFT plans are cached per
+ * (device, length, rows) for the life of the process. */
+
+/* d_x: n_rows rows of n_samples float32 (contiguous); d_out: same shape. */
+BP_API int bp_envelope_dev(const float *d_x, size_t n_rows, size_t n_samples, float clip_max,
+                           float *d_out, void *stream);
+
+/* Raw waveforms (S, C, T) to the beamformer's trace rows in one call: the
+ * envelope features of every (station, channel) row, then bp_prestack_dev
+ * with the same storage / layout arguments.  Replaces the tutorial's CPU
+ * feature loop followed by the reference front-end's CPU prestack
+ * (beampower/beampower.py:103-105). */
+BP_API int bp_prestack_envelope_dev(const float *d_waveforms, const float *d_weights_phases,
+                                    size_t n_samples, size_t n_stations, size_t n_channels,
+                                    size_t n_phases, float clip_max, int storage, size_t lpad,
+                                    size_t pitch, void *d_traces, float *d_scales,
+                                    void *stream);
 
 /* Host function: NumPy's float32 pairwise sum of x[0..n) (the summation
  * order the threshold kernels reproduce), for checking that order without a
