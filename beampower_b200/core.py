@@ -97,6 +97,8 @@ SIGNATURES = {
                        _vp], _int),
     "bp_pairwise_sum_f32": ([_vp, _sz], ct.c_float),
     "bp_envelope_dev": ([_vp, _sz, _sz, ct.c_float, _vp, _vp], _int),
+    "bp_seconds_to_samples_dev": ([_vp, _sz, _sz, ct.c_double, ct.c_double, _int, _vp, _vp],
+                                  _int),
     "bp_prestack_envelope_dev": ([_vp, _vp, _sz, _sz, _sz, _sz, ct.c_float, _int, _sz, _sz, _vp,
                                   _vp, _vp], _int),
     "bp_measure_peaks": ([_vp, ct.POINTER(ct.c_double), ct.POINTER(ct.c_double)], _int),

@@ -5,6 +5,7 @@
 // that the many kernel variants compile in parallel.
 #pragma once
 
+#include <algorithm>
 #include <atomic>
 #include <cstdint>
 #include <limits>

@@ -1,0 +1,79 @@
+// Travel times in seconds to integer sample delays, on the GPU: the
+// reference tutorial's sec_to_samp (notebooks/3_beampower.ipynb:378-393),
+// which turns the travel-time grid it reads from travel_times.h5 into the
+// int32 time_delays of beamform (:394), and the optional shift that makes
+// each source's delays relative to its earliest arrival (:396).
+//
+// The tutorial multiplies float32 seconds by a Python-float sampling rate,
+// so the arithmetic is float32: |t * sr| + epsilon, truncated to an integer,
+// with the sign of t restored.  Where that value is NaN, infinite or not
+// below 2^31 the tutorial's NumPy cast on x86 yields INT_MIN; so does this.
+#define BP_TEMPLATE_KERNELS_ONLY
+#include <climits>
+#include <cstdint>
+
+#include <cuda_runtime.h>
+
+#include "beampower_b200.h"
+#include "bp_host.h"
+
+using namespace bp_host;
+
+namespace {
+
+__global__ void seconds_to_samples_kernel(const float* __restrict__ t, long long n, float sr,
+                                          float eps, int32_t* __restrict__ out) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const float v = t[i];
+    const float a = __fadd_rn(fabsf(__fmul_rn(v, sr)), eps);
+    int32_t r;
+    if (!(a < 2147483648.0f)) {
+      r = INT_MIN;
+    } else {
+      const int32_t k = (int32_t)a;  // truncation toward zero (a >= 0)
+      r = v > 0.0f ? k : (v < 0.0f ? -k : 0);
+    }
+    out[i] = r;
+  }
+}
+
+// One warp per source: subtract the source's smallest delay (int32
+// arithmetic wraps, as NumPy's in-place subtract does).
+__global__ void relative_delays_kernel(int32_t* __restrict__ d, long long n_sources, int per) {
+  const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (gw >= n_sources) return;
+  int32_t* row = d + gw * per;
+  int32_t m = INT_MAX;
+  for (int j = lane; j < per; j += 32) m = min(m, row[j]);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = min(m, __shfl_xor_sync(0xFFFFFFFFu, m, o));
+  for (int j = lane; j < per; j += 32)
+    row[j] = (int32_t)((uint32_t)row[j] - (uint32_t)m);
+}
+
+}  // namespace
+
+extern "C" int bp_seconds_to_samples_dev(const float* d_seconds, size_t n_sources,
+                                         size_t n_per_source, double sampling_rate,
+                                         double epsilon, int relative, int32_t* d_delays,
+                                         void* stream) {
+  const size_t n = n_sources * n_per_source;
+  if (n == 0) return BP_OK;
+  if (!d_seconds || !d_delays) return fail(BP_ERR_INVALID_ARGUMENT, "NULL pointer");
+  if (n_per_source > (size_t)INT_MAX)
+    return fail(BP_ERR_UNSUPPORTED, "more than 2^31 - 1 delays per source");
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  const long long blocks = std::min<long long>(((long long)n + 255) / 256, 148LL * 16);
+  seconds_to_samples_kernel<<<(unsigned)blocks, 256, 0, st>>>(
+      d_seconds, (long long)n, (float)sampling_rate, (float)epsilon, d_delays);
+  BP_LAUNCHED("seconds_to_samples_kernel");
+  if (relative) {
+    const long long threads = (long long)n_sources * 32;
+    relative_delays_kernel<<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(
+        d_delays, (long long)n_sources, (int)n_per_source);
+    BP_LAUNCHED("relative_delays_kernel");
+  }
+  return BP_OK;
+}

@@ -113,6 +113,20 @@ class TravelTimeTable:
                                        _stream_ptr(stream)))
         return Traces(buf, scales, st, T, lpad, pitch)
 
+    @classmethod
+    def from_travel_times(cls, travel_times, sampling_rate, weights_sources, epsilon=0.2,
+                          relative=False, device=None):
+        """Table from travel times in seconds (N, S, P): the tutorial's
+        sec_to_samp conversion (notebooks/3_beampower.ipynb:378-396) on the
+        device, then the table build."""
+        from .ingest import sec_to_samp
+        _require_torch()
+        dev = device if device is not None else torch.device("cuda",
+                                                             torch.cuda.current_device())
+        tt = _dev_tensor(travel_times, torch.float32, dev)
+        return cls(sec_to_samp(tt, sampling_rate, epsilon, relative), weights_sources,
+                   device=dev)
+
     def traces_from_waveforms(self, waveforms, weights_phases, storage="fp32", clip_max=1e5,
                               stream=None):
         """Raw (S, C, T) waveforms to this table's trace layout in one device

@@ -54,7 +54,7 @@ def parse():
     ap.add_argument("--n-sources", type=int, default=None,
                     help="keep only the first n sources (profiling runs on a smaller case)")
     ap.add_argument("--storage", default="fp32", choices=["fp32", "bf16", "fp16"])
-    ap.add_argument("--workload", default="large", choices=["large", "batch", "serving"],
+    ap.add_argument("--workload", default="large", choices=["large", "batch", "serving", "stages"],
                     help="large: the 400k-source plain call (default); batch: 128 windows "
                          "in one persistent launch vs one call per window; serving: "
                          "8 streamed networks with Poisson chunk arrivals")
@@ -528,6 +528,9 @@ def main():
     if args.workload == "serving":
         run_serving(args, local_rank)
         return
+    if args.workload == "stages":
+        run_stages(args, local_rank)
+        return
     run_ours(args, rank, world, local_rank)
 
 
@@ -678,6 +681,131 @@ def run_serving(args, local_rank):
         "clocks": clocks,
     }
     print(json.dumps(line), flush=True)
+
+
+
+# ----------------------------------------------------------------------------
+# The stages either side of the beamformer (single GPU)
+# ----------------------------------------------------------------------------
+
+def run_stages(args, local_rank):
+    """The tutorial's steps before and after beamform_max, each at its
+    tutorial scale, device time (CUDA events) against the CPU code it
+    replaces:
+      features  -- envelope features of the 60-station x 3-channel x 180,000
+                   sample network, and raw waveforms to trace rows in one call;
+      detection -- threshold (rms, 7,200 s windows) and peaks (60 s apart)
+                   of a day-long 25 Hz beam series (2,160,000 samples);
+      ingest    -- 400,000 x 60 x 2 travel times (s) to relative delays."""
+    import torch
+    from scipy import signal
+    from oracle import detection as odet
+    from oracle import features as ofeat
+    from oracle import ingest as oing
+    from beampower_b200 import detection as det
+    from beampower_b200.features import envelope
+    from beampower_b200.ingest import sec_to_samp
+    from beampower_b200.tables import TravelTimeTable
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    hbm_peak = None
+    if os.path.exists(MEASURED_PEAKS):
+        with open(MEASURED_PEAKS) as fh:
+            hbm_peak = json.load(fh).get("hbm_gbs")
+    steps, warm = max(args.steps, 1), max(args.warmup, 3)
+    ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+
+    def gpu_ms(fn):
+        for _ in range(warm):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = ev(), ev()
+        e0.record()
+        for _ in range(steps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    def roof(bytes_, ms):
+        gbs = bytes_ / (ms * 1e-3) / 1e9
+        return {"bound": "hbm", "achieved": gbs, "peak": hbm_peak, "unit": "GB/s",
+                "frac": gbs / hbm_peak if hbm_peak else None,
+                "algorithmic_bytes": bytes_, "of": "measured (MEASURED_PEAKS.json)"}
+
+    rng = np.random.default_rng(0)
+    out = {}
+    sampler = ClockSampler(local_rank)
+    sampler.start()
+    time.sleep(0.3)
+    # ---- features ----
+    S, C, T, P = 60, 3, 180000, 2
+    w = torch.from_numpy(rng.standard_normal((S, C, T)).astype(np.float32)).to(dev)
+    A = torch.ones((S, C, P), device=dev)
+    ms_env = gpu_ms(lambda: envelope(w))
+    D = torch.zeros((64, S, P), dtype=torch.int32, device=dev)
+    table = TravelTimeTable(D, torch.ones((64, S), device=dev), device=dev)
+    ms_rows = gpu_ms(lambda: table.traces_from_waveforms(w, A))
+    table.close()
+    wc = w[:2].cpu().numpy()
+    t0 = time.perf_counter()
+    ofeat.waveform_features(wc)
+    cpu_env = (time.perf_counter() - t0) * (S / 2)
+    n = S * C * T
+    out["features"] = {
+        "samples": n, "envelope_ms": ms_env, "waveforms_to_trace_rows_ms": ms_rows,
+        "value": n / (ms_env * 1e-3), "unit": "samples/s",
+        "roofline": roof(8.0 * n, ms_env),
+        "cpu_baseline": {"value": n / cpu_env, "unit": "samples/s", "cores": 1, "kind": "port",
+                         "seconds": cpu_env,
+                         "sample": "tutorial envelope (SciPy) on 2 of 60 stations, scaled"}}
+    del w
+    # ---- detection ----
+    fs = 25.0
+    nd = int(24 * 3600 * fs)
+    x = np.abs(rng.standard_normal(nd + 24)).astype(np.float32)
+    x = np.convolve(x, np.ones(25, np.float32) / 25, mode="valid")[:nd].astype(np.float32)
+    x[nd - 2864:] = 0.0
+    Wn, dist = int(7200 * fs), int(60 * fs)
+    noise = rng.standard_normal(2864).astype(np.float32)
+    xt = torch.from_numpy(x).to(dev)
+    nt = torch.from_numpy(noise).to(dev)
+    ms_thr = gpu_ms(lambda: det.time_dependent_threshold(xt, Wn, 0.66, "rms", 8.0,
+                                                         white_noise=nt))
+    thr = det.time_dependent_threshold(xt, Wn, 0.66, "rms", 8.0, white_noise=nt)
+    ms_det = gpu_ms(lambda: det.detect(xt, threshold=thr, distance=dist))
+    t0 = time.perf_counter()
+    thr_c = odet.time_dependent_threshold(x, Wn, 0.66, "rms", 8.0, noise)
+    t1 = time.perf_counter()
+    pk = signal.find_peaks(x, distance=dist)[0]
+    pk = pk[x[pk] > thr_c[pk]]
+    t2 = time.perf_counter()
+    out["detection"] = {
+        "samples": nd, "threshold_ms": ms_thr, "detect_ms": ms_det,
+        "value": nd / ((ms_thr + ms_det) * 1e-3), "unit": "samples/s",
+        "detections": int(pk.size),
+        "roofline": roof(16.0 * nd, ms_thr + ms_det),
+        "note": "host-synchronised rounds (counts read back): latency bound, not HBM bound",
+        "cpu_baseline": {"value": nd / (t2 - t0), "unit": "samples/s", "cores": 1,
+                         "kind": "port", "seconds": t2 - t0, "threshold_s": t1 - t0,
+                         "sample": "the whole series: tutorial threshold (NumPy) + "
+                                   "scipy.signal.find_peaks"}}
+    # ---- ingest ----
+    tt = rng.uniform(0.0, 40.0, size=(400000, 60, 2)).astype(np.float32)
+    ttd = torch.from_numpy(tt).to(dev)
+    ms_ing = gpu_ms(lambda: sec_to_samp(ttd, 50.0, relative=True))
+    t0 = time.perf_counter()
+    oing.sec_to_samp(tt, 50.0, relative=True)
+    cpu_ing = time.perf_counter() - t0
+    ni = tt.size
+    out["ingest"] = {
+        "values": ni, "ms": ms_ing, "value": ni / (ms_ing * 1e-3), "unit": "delays/s",
+        "roofline": roof(8.0 * ni, ms_ing),
+        "cpu_baseline": {"value": ni / cpu_ing, "unit": "delays/s", "cores": 1, "kind": "port",
+                         "seconds": cpu_ing, "sample": "the whole grid (NumPy)"}}
+    clocks = sampler.stop()
+    print(json.dumps({"workload": "stages", "n_gpus": 1, "steps": steps, "warmup": warm,
+                      "data": "synthetic", "stages": out, "clocks": clocks}), flush=True)
 
 
 if __name__ == "__main__":

@@ -3,7 +3,8 @@
  * (beampower_b200/lib/libbeampower_b200.so).
  *
  * Four groups of entry points; groups 3 (detection on the beam series) and
- * 4 (waveform features) are described at their sections below:
+ * 4 (inputs: waveform features, travel times in samples) are described at
+ * their sections below:
  *
  * 1. Drop-ins for the reference's GPU library.  Same symbol names, argument
  *    order and meaning as beampower/src/beamform_gpu.h:1-2, bound by
@@ -334,7 +335,7 @@ BP_API int bp_detect_dev(const float *d_beam_max, const int32_t *d_argmax,
                          size_t capacity, size_t *n_detections, void *stream);
 
 /* ======================================================================= */
-/* 4. Waveform features (the step before the prestack)                      */
+/* 4. Inputs: waveform features and travel times in samples              */
 /* ======================================================================= */
 /* The reference tutorial's envelope transform (notebooks/3_beampower.ipynb:
  * 74-103, `envelope`, applied to every trace at :145-147): the modulus of the
@@ -359,6 +360,18 @@ BP_API int bp_prestack_envelope_dev(const float *d_waveforms, const float *d_wei
                                     size_t n_phases, float clip_max, int storage, size_t lpad,
                                     size_t pitch, void *d_traces, float *d_scales,
                                     void *stream);
+
+/* Travel times in seconds to int32 sample delays, as the tutorial's
+ * sec_to_samp (notebooks/3_beampower.ipynb:378-394): in float32,
+ * sign(t) * trunc(|t * sampling_rate| + epsilon) (epsilon 0.2 there), and
+ * INT_MIN where that is NaN, infinite or not below 2^31 (the x86 result of
+ * the tutorial's NumPy cast).  d_seconds and d_delays hold n_sources rows of
+ * n_per_source values ((S, P) per source); relative != 0 then subtracts each
+ * row's minimum, the tutorial's optional relative delays (:396).  Reading
+ * the tutorial's travel_times.h5 stays with the caller. */
+BP_API int bp_seconds_to_samples_dev(const float *d_seconds, size_t n_sources,
+                                     size_t n_per_source, double sampling_rate, double epsilon,
+                                     int relative, int32_t *d_delays, void *stream);
 
 /* Host function: NumPy's float32 pairwise sum of x[0..n) (the summation
  * order the threshold kernels reproduce), for checking that order without a
