@@ -21,36 +21,36 @@ using namespace bp_host;
 
 namespace {
 
+__device__ __forceinline__ int32_t seconds_to_samples(float v, float sr, float eps) {
+  const float a = __fadd_rn(fabsf(__fmul_rn(v, sr)), eps);
+  if (!(a < 2147483648.0f)) return INT_MIN;
+  const int32_t k = (int32_t)a;  // truncation toward zero (a >= 0)
+  return v > 0.0f ? k : (v < 0.0f ? -k : 0);
+}
+
 __global__ void seconds_to_samples_kernel(const float* __restrict__ t, long long n, float sr,
                                           float eps, int32_t* __restrict__ out) {
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (long long)gridDim.x * blockDim.x) {
-    const float v = t[i];
-    const float a = __fadd_rn(fabsf(__fmul_rn(v, sr)), eps);
-    int32_t r;
-    if (!(a < 2147483648.0f)) {
-      r = INT_MIN;
-    } else {
-      const int32_t k = (int32_t)a;  // truncation toward zero (a >= 0)
-      r = v > 0.0f ? k : (v < 0.0f ? -k : 0);
-    }
-    out[i] = r;
-  }
+       i += (long long)gridDim.x * blockDim.x)
+    out[i] = seconds_to_samples(t[i], sr, eps);
 }
 
-// One warp per source: subtract the source's smallest delay (int32
-// arithmetic wraps, as NumPy's in-place subtract does).
-__global__ void relative_delays_kernel(int32_t* __restrict__ d, long long n_sources, int per) {
+// One warp per source: convert, then subtract the source's smallest delay
+// (int32 arithmetic wraps, as NumPy's in-place subtract does).  The row is
+// read twice; the second read comes from cache.
+__global__ void relative_delays_kernel(const float* __restrict__ t, long long n_sources, int per,
+                                       float sr, float eps, int32_t* __restrict__ d) {
   const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (gw >= n_sources) return;
-  int32_t* row = d + gw * per;
+  const float* row = t + gw * per;
+  int32_t* out = d + gw * per;
   int32_t m = INT_MAX;
-  for (int j = lane; j < per; j += 32) m = min(m, row[j]);
+  for (int j = lane; j < per; j += 32) m = min(m, seconds_to_samples(row[j], sr, eps));
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) m = min(m, __shfl_xor_sync(0xFFFFFFFFu, m, o));
   for (int j = lane; j < per; j += 32)
-    row[j] = (int32_t)((uint32_t)row[j] - (uint32_t)m);
+    out[j] = (int32_t)((uint32_t)seconds_to_samples(row[j], sr, eps) - (uint32_t)m);
 }
 
 }  // namespace
@@ -65,15 +65,17 @@ extern "C" int bp_seconds_to_samples_dev(const float* d_seconds, size_t n_source
   if (n_per_source > (size_t)INT_MAX)
     return fail(BP_ERR_UNSUPPORTED, "more than 2^31 - 1 delays per source");
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-  const long long blocks = std::min<long long>(((long long)n + 255) / 256, 148LL * 16);
-  seconds_to_samples_kernel<<<(unsigned)blocks, 256, 0, st>>>(
-      d_seconds, (long long)n, (float)sampling_rate, (float)epsilon, d_delays);
-  BP_LAUNCHED("seconds_to_samples_kernel");
+  const float sr = (float)sampling_rate, eps = (float)epsilon;
   if (relative) {
     const long long threads = (long long)n_sources * 32;
     relative_delays_kernel<<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(
-        d_delays, (long long)n_sources, (int)n_per_source);
+        d_seconds, (long long)n_sources, (int)n_per_source, sr, eps, d_delays);
     BP_LAUNCHED("relative_delays_kernel");
+    return BP_OK;
   }
+  const long long blocks = std::min<long long>(((long long)n + 255) / 256, 148LL * 16);
+  seconds_to_samples_kernel<<<(unsigned)blocks, 256, 0, st>>>(d_seconds, (long long)n, sr, eps,
+                                                              d_delays);
+  BP_LAUNCHED("seconds_to_samples_kernel");
   return BP_OK;
 }
