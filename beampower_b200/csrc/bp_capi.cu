@@ -57,6 +57,21 @@ int device_smem_optin(int dev) {
   return v;
 }
 
+// Keeps the device's default stream-ordered pool from returning memory to
+// the driver at every synchronisation (cudaMallocAsync scratch is reused).
+void retain_pool(int dev) {
+  static std::atomic<uint64_t> done{0};
+  if (dev < 0 || dev >= 64) return;
+  const uint64_t bit = 1ull << dev;
+  if (done.load() & bit) return;
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+    uint64_t thr = std::numeric_limits<uint64_t>::max();
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+  }
+  done.fetch_or(bit);
+}
+
 }  // namespace bp_host
 
 using namespace bp_host;
@@ -143,18 +158,6 @@ size_t pad256(size_t v) { return (v + 255) / 256 * 256; }
 // Keep freed stream-ordered allocations in the device's default pool between
 // calls (the default release threshold hands them back to the driver at every
 // synchronisation, and re-mapping hundreds of MB costs tens of ms per call).
-void retain_pool(int dev) {
-  static std::atomic<uint64_t> done{0};
-  if (dev < 0 || dev >= 64) return;
-  const uint64_t bit = 1ull << dev;
-  if (done.load() & bit) return;
-  cudaMemPool_t pool;
-  if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
-    uint64_t thr = std::numeric_limits<uint64_t>::max();
-    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
-  }
-  done.fetch_or(bit);
-}
 
 bool tiling_map_enabled() {
   const char* v = std::getenv("BEAMPOWER_B200_TILING_MAP");

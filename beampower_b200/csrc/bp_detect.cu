@@ -184,7 +184,7 @@ int pw_mean(const float* x, long long seg_stride, int len, int n_seg, int mode,
   pw_leaves_kernel<<<g1, 128, 0, st>>>(x, seg_stride, mode, centre, d_leaves, nl, t.n_nodes,
                                        n_seg, vals);
   BP_LAUNCHED("pw_leaves_kernel");
-  pw_inner_kernel<<<(unsigned)std::min(n_seg, 65535), 256, 0, st>>>(
+  pw_inner_kernel<<<(unsigned)std::min(n_seg, 65535), n_seg == 1 ? 1024 : 256, 0, st>>>(
       d_inner, d_levels, (int)t.level_end.size(), t.n_nodes, t.root, len, n_seg, vals, out);
   BP_LAUNCHED("pw_inner_kernel");
   return BP_OK;

@@ -98,21 +98,22 @@ int fft_inverse_c2c(int n, int batch, cufftComplex* data, cudaStream_t st) {
   return BP_OK;
 }
 
-// Full-length analytic spectrum from the half spectrum of a real row.
-__global__ void hilbert_weights_kernel(const cufftComplex* __restrict__ half, int n, int rows,
+// Full-length analytic spectrum from the half spectrum of a real row
+// (grid: x over the row's bins, y over rows).
+__global__ void hilbert_weights_kernel(const cufftComplex* __restrict__ half, int n,
                                        cufftComplex* __restrict__ full) {
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= (long long)n * rows) return;
-  const int r = (int)(i / n), k = (int)(i % n);
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const size_t r = blockIdx.y;
   const int nh = n / 2 + 1;
   cufftComplex z = make_cuFloatComplex(0.0f, 0.0f);
   if (k == 0 || (n % 2 == 0 && k == n / 2)) {
-    z = half[(size_t)r * nh + k];
+    z = half[r * nh + k];
   } else if (k < (n + 1) / 2) {
-    const cufftComplex x = half[(size_t)r * nh + k];
+    const cufftComplex x = half[r * nh + k];
     z = make_cuFloatComplex(2.0f * x.x, 2.0f * x.y);
   }
-  full[i] = z;
+  full[r * n + k] = z;
 }
 
 // Envelope = |inverse transform| / n.
@@ -129,17 +130,18 @@ __device__ __forceinline__ float clip_above(float x, float hi) {
   return (isnan(x) || x <= hi) ? x : hi;
 }
 
-// (env - median) / (mad, or 1 when it is 0), clipped above.
-__global__ void normalise_kernel(const float* __restrict__ env, int n, int rows,
+// (env - median) / (mad, or 1 when it is 0), clipped above (grid: x over
+// the row's samples, y over rows).
+__global__ void normalise_kernel(const float* __restrict__ env, int n,
                                  const float* __restrict__ med, const float* __restrict__ mad,
                                  float clip_max, long long out_pitch, float* __restrict__ out) {
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= (long long)n * rows) return;
-  const int r = (int)(i / n), k = (int)(i % n);
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const size_t r = blockIdx.y;
   const float m = mad[r];
   const float scale = m == 0.0f ? 1.0f : m;
-  out[(size_t)r * out_pitch + k] = clip_above(__fdiv_rn(__fsub_rn(env[i], med[r]), scale),
-                                              clip_max);
+  out[r * out_pitch + k] = clip_above(__fdiv_rn(__fsub_rn(env[r * n + k], med[r]), scale),
+                                      clip_max);
 }
 
 // Rows per pass so that the two complex buffers stay within a few GB.
@@ -173,16 +175,16 @@ int envelope_rows(const float* x, size_t rows, size_t n, size_t in_pitch, float 
                               n * sizeof(float), b, cudaMemcpyDeviceToDevice, st));
     BP_TRY(fft_forward_r2c(N, b, re, half, st));
     const long long count = (long long)b * N;
-    hilbert_weights_kernel<<<grid_for(count, 256), 256, 0, st>>>(half, N, b, full);
+    const dim3 rows_grid((unsigned)((N + 255) / 256), (unsigned)b);
+    hilbert_weights_kernel<<<rows_grid, 256, 0, st>>>(half, N, full);
     BP_LAUNCHED("hilbert_weights_kernel");
     BP_TRY(fft_inverse_c2c(N, b, full, st));
     modulus_kernel<<<grid_for(count, 256), 256, 0, st>>>(full, count, 1.0f / (float)N, env);
     BP_LAUNCHED("modulus_kernel");
     BP_TRY(np_median(env, N, N, b, 0, nullptr, med, sc, st));
     BP_TRY(np_median(env, N, N, b, 1, med, mad, sc, st));
-    normalise_kernel<<<grid_for(count, 256), 256, 0, st>>>(env, N, b, med, mad, clip_max,
-                                                           (long long)out_pitch,
-                                                           out + r0 * out_pitch);
+    normalise_kernel<<<rows_grid, 256, 0, st>>>(env, N, med, mad, clip_max, (long long)out_pitch,
+                                                out + r0 * out_pitch);
     BP_LAUNCHED("normalise_kernel");
   }
   return BP_OK;

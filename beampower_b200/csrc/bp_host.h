@@ -26,6 +26,9 @@ extern std::atomic<uint64_t> g_launches;
 
 int device_sm_count(int dev);
 int device_smem_optin(int dev);
+// Raises the release threshold of the device's default memory pool once, so
+// cudaMallocAsync scratch stays mapped between calls.
+void retain_pool(int dev);
 
 constexpr long long kMaxInt = std::numeric_limits<int>::max();
 

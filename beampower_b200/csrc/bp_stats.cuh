@@ -25,7 +25,10 @@ constexpr unsigned kFull = 0xFFFFFFFFu;
 struct Scratch {
   cudaStream_t st;
   std::vector<void*> ptrs;
-  explicit Scratch(cudaStream_t s) : st(s) {}
+  explicit Scratch(cudaStream_t s) : st(s) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess) retain_pool(dev);
+  }
   ~Scratch() {
     for (void* p : ptrs) cudaFreeAsync(p, st);
   }
@@ -95,85 +98,123 @@ __global__ void select_init_kernel(SelState* st, int n_seg, int len) {
   st[w] = s;
 }
 
-// Histogram of the next 8 bits of the values whose higher bits match each
-// statistic's prefix.  mode 1 selects among |x - centre[w]| (float32).
+// Radix digits, most significant first.  Wide digits (12 + 10 + 10 bits)
+// spread the first pass over many bins -- the values of one row share few
+// exponents, and 8-bit first digits put almost all of them in a handful of
+// bins whose shared atomics then serialise -- and need one pass fewer; they
+// are used while the per-segment histograms (4096 bins) stay small in total.
+struct Digit {
+  int shift, width;
+};
+constexpr Digit kWideDigits[3] = {{20, 12}, {10, 10}, {0, 10}};
+constexpr Digit kByteDigits[4] = {{24, 8}, {16, 8}, {8, 8}, {0, 8}};
+constexpr int kWideBins = 4096;
+
+// Histogram of the current digit of the values whose higher bits match each
+// statistic's prefix (dynamic shared memory: 2 x bins counters).  mode 1
+// selects among |x - centre[w]| (float32).
 __global__ void __launch_bounds__(256)
 select_hist_kernel(const float* __restrict__ x, long long seg_stride, int len, int mode,
-                   const float* __restrict__ centre, int n_seg, int pass,
-                   SelState* __restrict__ st, unsigned* __restrict__ hist) {
-  __shared__ unsigned h[2][256];
+                   const float* __restrict__ centre, int n_seg, Digit dg, int first,
+                   int hist_stride, SelState* __restrict__ st, unsigned* __restrict__ hist) {
+  extern __shared__ unsigned h[];  // [2][bins]
   __shared__ unsigned nan_count;
-  const int shift = 24 - 8 * pass;
-  const uint32_t mask = pass == 0 ? 0u : (0xFFFFFFFFu << (32 - 8 * pass));
+  const int bins = 1 << dg.width;
+  const int top = dg.shift + dg.width;
+  const uint32_t mask = top >= 32 ? 0u : (0xFFFFFFFFu << top);
   for (int w = blockIdx.y; w < n_seg; w += gridDim.y) {
-    for (int b = threadIdx.x; b < 512; b += blockDim.x) (&h[0][0])[b] = 0;
+    const int q = st[w].q;
+    for (int b = threadIdx.x; b < bins * q; b += blockDim.x) h[b] = 0;
     if (threadIdx.x == 0) nan_count = 0;
     __syncthreads();
-    const int q = st[w].q;
     const uint32_t p0 = st[w].prefix[0] & mask, p1 = st[w].prefix[1] & mask;
+    // the two middle ranks of an even length usually share their prefix:
+    // then one histogram serves both
+    const bool shared_prefix = q == 2 && p0 == p1;
+    const bool second = q == 2 && !shared_prefix;
     const float c = mode ? centre[w] : 0.0f;
     const float* base = x + (size_t)w * seg_stride;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < len;
-         i += (long long)gridDim.x * blockDim.x) {
-      float v = base[i];
-      if (mode) v = fabsf(__fsub_rn(v, c));
-      if (pass == 0 && isnan(v)) atomicAdd(&nan_count, 1u);
-      const uint32_t key = order_key(v);
-      const uint32_t bin = (key >> shift) & 255u;
-      if ((key & mask) == p0) atomicAdd(&h[0][bin], 1u);
-      if (q == 2 && (key & mask) == p1) atomicAdd(&h[1][bin], 1u);
+    // eight independent loads per thread before the atomics (the atomics
+    // would otherwise keep one load in flight per thread)
+    constexpr int U = 8;
+    const long long step = (long long)gridDim.x * blockDim.x * U;
+    for (long long i0 = (long long)blockIdx.x * blockDim.x * U + threadIdx.x; i0 < len;
+         i0 += step) {
+      float v[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const long long i = i0 + (long long)u * blockDim.x;
+        v[u] = i < len ? base[i] : 0.0f;
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        if (i0 + (long long)u * blockDim.x >= len) break;
+        float y = v[u];
+        if (mode) y = fabsf(__fsub_rn(y, c));
+        if (first && isnan(y)) atomicAdd(&nan_count, 1u);
+        const uint32_t key = order_key(y);
+        const uint32_t bin = (key >> dg.shift) & (uint32_t)(bins - 1);
+        if ((key & mask) == p0) atomicAdd(&h[bin], 1u);
+        if (second && (key & mask) == p1) atomicAdd(&h[bins + bin], 1u);
+      }
     }
     __syncthreads();
-    for (int b = threadIdx.x; b < 256 * q; b += blockDim.x) {
-      const unsigned v = (&h[0][0])[b];
-      if (v) atomicAdd(&hist[(size_t)w * 512 + b], v);
+    unsigned* g = hist + (size_t)w * 2 * hist_stride;
+    for (int b = threadIdx.x; b < bins * q; b += blockDim.x) {
+      const int qi = b / bins, bin = b % bins;
+      const unsigned v = (shared_prefix && qi == 1) ? h[bin] : h[b];
+      if (v) atomicAdd(&g[(size_t)qi * hist_stride + bin], v);
     }
     if (threadIdx.x == 0 && nan_count) atomicAdd(&st[w].nan, nan_count);
     __syncthreads();
   }
 }
 
-// One warp per (segment, statistic): the bin that holds the wanted rank
-// becomes the next 8 bits of its prefix; the histogram is cleared.
-__global__ void select_pick_kernel(SelState* __restrict__ st, unsigned* __restrict__ hist,
-                                   int n_seg, int pass) {
-  const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  const long long w = gw >> 1;
-  const int qi = (int)(gw & 1);
-  if (w >= n_seg) return;
-  unsigned* h = hist + (size_t)w * 512 + qi * 256;
-  if (qi < st[w].q) {
-    unsigned c[8], tot = 0;
+// One 256-thread block per (segment, statistic): thread t owns bins
+// [t * per, (t + 1) * per); a block-wide exclusive scan of the per-thread
+// totals locates the bin that holds the wanted rank, which becomes the next
+// digit of the prefix.  The histogram is cleared for the next pass.
+__global__ void __launch_bounds__(256)
+select_pick_kernel(SelState* __restrict__ st, unsigned* __restrict__ hist, int n_seg, Digit dg,
+                   int hist_stride) {
+  __shared__ unsigned warp_tot[8];
+  const int w = blockIdx.x >> 1, qi = blockIdx.x & 1;
+  if (w >= n_seg || qi >= st[w].q) return;  // block-uniform
+  const int bins = 1 << dg.width;
+  const int per = bins / 256;  // 16 (wide digits) or 1
+  const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
+  unsigned* h = hist + (size_t)w * 2 * hist_stride + (size_t)qi * hist_stride + (size_t)t * per;
+  unsigned c[16];
+  unsigned tot = 0;
+  for (int j = 0; j < per; ++j) {
+    c[j] = h[j];
+    tot += c[j];
+  }
+  unsigned incl = tot;
 #pragma unroll
-    for (int j = 0; j < 8; ++j) {
-      c[j] = h[lane * 8 + j];
-      tot += c[j];
-    }
-    unsigned incl = tot;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const unsigned v = __shfl_up_sync(kFull, incl, o);
-      if (lane >= o) incl += v;
-    }
-    const unsigned excl = incl - tot;
-    const uint32_t r = st[w].rank[qi];
-    if (r >= excl && r < incl) {
-      unsigned acc = excl;
-      for (int j = 0; j < 8; ++j) {
-        if (r < acc + c[j]) {
-          const int shift = 24 - 8 * pass;
-          st[w].prefix[qi] |= (uint32_t)(lane * 8 + j) << shift;
-          st[w].rank[qi] = r - acc;
-          break;
-        }
-        acc += c[j];
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned v = __shfl_up_sync(kFull, incl, o);
+    if (lane >= o) incl += v;
+  }
+  if (lane == 31) warp_tot[wid] = incl;
+  __syncthreads();
+  unsigned before = 0;
+  for (int k = 0; k < wid; ++k) before += warp_tot[k];
+  const unsigned excl = before + incl - tot;
+  const uint32_t r = st[w].rank[qi];
+  __syncthreads();  // every thread has read rank before it changes
+  if (r >= excl && r < excl + tot) {
+    unsigned acc = excl;
+    for (int j = 0; j < per; ++j) {
+      if (r < acc + c[j]) {
+        st[w].prefix[qi] |= (uint32_t)(t * per + j) << dg.shift;
+        st[w].rank[qi] = r - acc;
+        break;
       }
+      acc += c[j];
     }
   }
-  __syncwarp();
-#pragma unroll
-  for (int j = 0; j < 8; ++j) h[lane * 8 + j] = 0;
+  for (int j = 0; j < per; ++j) h[j] = 0;
 }
 
 // NumPy's median from the order statistics: NaN if any NaN, else the middle
@@ -197,22 +238,28 @@ __global__ void select_finish_kernel(const SelState* __restrict__ st, int n_seg,
 
 int np_median(const float* x, long long seg_stride, int len, int n_seg, int mode,
               const float* centre, float* out, Scratch& sc, cudaStream_t st) {
+  const bool wide = (long long)n_seg * 2 * kWideBins <= (1LL << 24);  // <= 64 MB of counters
+  const int n_pass = wide ? 3 : 4;
+  const Digit* digits = wide ? kWideDigits : kByteDigits;
+  const int hist_stride = wide ? kWideBins : 256;
   SelState* state = nullptr;
   unsigned* hist = nullptr;
   BP_TRY(sc.get(&state, n_seg));
-  BP_TRY(sc.get(&hist, (size_t)n_seg * 512));
-  BP_CUDA(cudaMemsetAsync(hist, 0, (size_t)n_seg * 512 * sizeof(unsigned), st));
+  BP_TRY(sc.get(&hist, (size_t)n_seg * 2 * hist_stride));
+  BP_CUDA(cudaMemsetAsync(hist, 0, (size_t)n_seg * 2 * hist_stride * sizeof(unsigned), st));
   select_init_kernel<<<grid_for(n_seg, 256), 256, 0, st>>>(state, n_seg, len);
   BP_LAUNCHED("select_init_kernel");
   if (len > 0) {
-    const unsigned gx = grid_for(len, 256 * 16, 1024);
+    const unsigned gx = grid_for(len, 256 * 64, 1024);
     dim3 g(gx, (unsigned)std::min(n_seg, 65535));
-    for (int pass = 0; pass < 4; ++pass) {
-      select_hist_kernel<<<g, 256, 0, st>>>(x, seg_stride, len, mode, centre, n_seg, pass, state,
-                                            hist);
+    const size_t smem = 2 * (size_t)hist_stride * sizeof(unsigned);
+    for (int pass = 0; pass < n_pass; ++pass) {
+      select_hist_kernel<<<g, 256, smem, st>>>(x, seg_stride, len, mode, centre, n_seg,
+                                               digits[pass], pass == 0 ? 1 : 0, hist_stride,
+                                               state, hist);
       BP_LAUNCHED("select_hist_kernel");
-      select_pick_kernel<<<grid_for((long long)n_seg * 64, 256), 256, 0, st>>>(state, hist,
-                                                                               n_seg, pass);
+      select_pick_kernel<<<(unsigned)(2 * n_seg), 256, 0, st>>>(state, hist, n_seg,
+                                                                 digits[pass], hist_stride);
       BP_LAUNCHED("select_pick_kernel");
     }
   }
