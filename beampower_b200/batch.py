@@ -22,7 +22,7 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from .core import STORAGE, Record, check, load_library
+from .core import STORAGE, Record, check, load_library, trace_copies
 from .tables import TravelTimeTable, _dev_tensor, _stream_ptr
 
 try:
@@ -92,7 +92,7 @@ class WindowBatch:
             if tab.n_stations != S or tab.n_phases != P:
                 raise ValueError("window tables must match weights_phases")
             lpad, pitch = tab.layout(w.n_samples)
-            rows = S * P * (1 if st == 0 else 2)
+            rows = S * P * trace_copies(st)
             self.features.append(torch.zeros((S, C, w.n_samples), dtype=torch.float32,
                                              device=self.device))
             self.traces.append(torch.empty((rows, pitch), dtype=elem, device=self.device))

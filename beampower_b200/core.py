@@ -96,6 +96,7 @@ SIGNATURES = {
     "bp_detect_dev": ([_vp, _vp, _vp, _sz, ct.c_double, _vp, _vp, _vp, _sz, ct.POINTER(_sz),
                        _vp], _int),
     "bp_pairwise_sum_f32": ([_vp, _sz], ct.c_float),
+    "bp_trace_copies": ([_int], _int),
     "bp_envelope_dev": ([_vp, _sz, _sz, ct.c_float, _vp, _vp], _int),
     "bp_seconds_to_samples_dev": ([_vp, _sz, _sz, ct.c_double, ct.c_double, _int, _vp, _vp],
                                   _int),
@@ -194,3 +195,11 @@ def check(status: int) -> None:
 def launch_count() -> int:
     """Kernel launches issued by the library in this process."""
     return int(load_library("gpu").bp_launch_count())
+
+
+def trace_copies(storage: int) -> int:
+    """Rows per (station, phase) of trace storage (1 FP32, 4 for 16-bit)."""
+    n = load_library("gpu").bp_trace_copies(int(storage))
+    if n < 1:
+        raise ValueError(f"unknown storage {storage}")
+    return n

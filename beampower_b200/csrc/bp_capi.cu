@@ -274,13 +274,17 @@ int launch_window(int cfg, int P, bool checked, int storage, const bp::LaunchArg
 }
 
 template <int CFG>
-size_t staged_smem_cfg(int P, bool maxred, int rowcap, int max_active) {
+size_t staged_smem_cfg(int P, bool maxred, int rowcap, int max_active, int row_factor) {
   using C = KCfg<CFG>;
   auto f = [&](auto tag) -> size_t {
     constexpr int PP = decltype(tag)::value;
     if (maxred)
-      return bp::WindowSmem<PP, C::KS, C::MT, C::WS, C::NSTAGE, true>(rowcap, max_active).total;
-    return bp::WindowSmem<PP, C::KS, C::MT, C::WS, C::NSTAGE, false>(rowcap, max_active).total;
+      return bp::WindowSmem<PP, C::KS, C::MT, C::WS, C::NSTAGE, true>(rowcap, max_active,
+                                                                       row_factor)
+          .total;
+    return bp::WindowSmem<PP, C::KS, C::MT, C::WS, C::NSTAGE, false>(rowcap, max_active,
+                                                                      row_factor)
+        .total;
   };
   switch (P) {
     case 1: return f(std::integral_constant<int, 1>{});
@@ -291,9 +295,12 @@ size_t staged_smem_cfg(int P, bool maxred, int rowcap, int max_active) {
   return SIZE_MAX;
 }
 
-size_t staged_smem_bytes(int cfg, int P, bool maxred, int rowcap, int max_active) {
-  if (cfg == 1) return staged_smem_cfg<1>(P, maxred, rowcap, max_active);
-  return staged_smem_cfg<0>(P, maxred, rowcap, max_active);
+// Shared memory of the staged kernel; storage < 0: the largest over storages.
+size_t staged_smem_bytes(int cfg, int P, bool maxred, int rowcap, int max_active, int storage) {
+  const int rf = storage == BP_STORAGE_F32 ? bp::ring_row_factor<BP_STORAGE_F32>()
+                                           : bp::ring_row_factor<BP_STORAGE_F16>();
+  if (cfg == 1) return staged_smem_cfg<1>(P, maxred, rowcap, max_active, rf);
+  return staged_smem_cfg<0>(P, maxred, rowcap, max_active, rf);
 }
 
 int rowcap_for(const bp_table* t, int cfg) {
@@ -305,7 +312,7 @@ int rowcap_for(const bp_table* t, int cfg) {
 int config_for(const bp_table* t, int storage, bool maxred) {
   const int c = pick_config(storage, maxred);
   if (c != 0 && staged_smem_bytes(c, t->dev.P, maxred, rowcap_for(t, c),
-                                  std::max(1, t->info.max_active)) >
+                                  std::max(1, t->info.max_active), storage) >
                      (size_t)device_smem_optin(t->device))
     return 0;
   return c;
@@ -612,7 +619,8 @@ int bp_table_create(const int32_t* d_delays, const float* d_weights, size_t N, s
   if (use_window) {
     const int rowcap = (int)bp::align_up_sz((size_t)(cfg_time_tile(0) + in.max_spread + 1),
                                             bp::kAlign);
-    const size_t need = staged_smem_bytes(0, (int)P, true, rowcap, std::max(1, in.max_active));
+    // sized for the largest storage, so that the choice holds for every call
+    const size_t need = staged_smem_bytes(0, (int)P, true, rowcap, std::max(1, in.max_active), -1);
     if (need > (size_t)device_smem_optin(t->device)) use_window = false;
   }
   in.uses_window_kernel = use_window ? 1 : 0;
@@ -844,10 +852,10 @@ int host_path(cudaStream_t st, DevBufs& bufs, const int32_t* d_delays, const flo
   if (int rc = bp_table_create(d_delays, d_w, N, S, P, st, &tg.t)) return rc;
   size_t lpad = 0, pitch = 0;
   if (int rc = bp_trace_layout(tg.t, T, &lpad, &pitch)) return rc;
-  // FP32: S*P rows of 4-byte elements; 16-bit: 2*S*P rows of 2-byte elements
+  // FP32: S*P rows of 4-byte elements; 16-bit: kHalfCopies*S*P rows of 2 bytes
   void* d_traces = nullptr;
   float* d_scales = nullptr;
-  BP_CUDA(bufs.alloc(&d_traces, S * P * pitch * 4));
+  BP_CUDA(bufs.alloc(&d_traces, S * P * pitch * (storage == BP_STORAGE_F32 ? 4 : 2 * bp::kHalfCopies)));
   BP_CUDA(bufs.alloc(&d_scales, S * sizeof(float)));
   if (int rc = traces_fill(d_traces, d_scales, lpad, pitch)) return rc;
   if (reduce == BP_REDUCE_MAX) {
@@ -1337,6 +1345,13 @@ int bp_record_beamform_max_dev(const bp_table* t, const bp_record* q, int storag
 }  // extern "C"
 
 extern "C" {
+
+int bp_trace_copies(int storage) {
+  if (storage == BP_STORAGE_F32) return 1;
+  if (storage == BP_STORAGE_BF16 || storage == BP_STORAGE_F16) return bp::kHalfCopies;
+  fail(BP_ERR_INVALID_ARGUMENT, "unknown storage %d", storage);
+  return -1;
+}
 
 int bp_kernel_config_count(void) { return kNumConfigs; }
 

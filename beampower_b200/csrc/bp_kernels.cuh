@@ -28,6 +28,16 @@ namespace bp {
 // Window starts are aligned down to this many samples (32 bytes of FP32,
 // 16 bytes of 16-bit storage), so every bulk copy starts 16-byte aligned.
 constexpr int kAlign = 8;
+// 16-bit trace storage keeps this many copies of every row, copy v shifted
+// by v samples, so that any run of 4 samples is one 8-byte-aligned pair of
+// 32-bit words in one of the copies (one 64-bit shared load per lane).
+constexpr int kHalfCopies = 4;
+// 32-bit words of one ring row per sample of window capacity: FP32 1, 16-bit
+// 2 (kHalfCopies copies of 2-byte elements).
+template <int STORAGE>
+constexpr int ring_row_factor() {
+  return STORAGE == BP_STORAGE_F32 ? 1 : kHalfCopies / 2;
+}
 // Largest time tile of any kernel configuration; trace layouts are padded
 // for it so that one layout serves every configuration.
 constexpr int kMaxTimeTile = 1024;
@@ -242,7 +252,7 @@ struct TableView {
 // Sample t of the record is global sample t_origin + t.  Traces hold samples
 // [0, T) (zeros outside); results are produced for samples [out0, out1).
 struct RecordView {
-  const void* traces;   // FP32 rows, or 16-bit rows in two versions (see Half16)
+  const void* traces;   // FP32 rows, or 16-bit rows in kHalfCopies shifted copies
   const float* scales;  // per-station scale of 16-bit storage (unused for FP32)
   long long pitch;      // elements per row
   long long t_origin;   // global index of record sample 0 (strict lower bound)
@@ -294,9 +304,11 @@ struct WindowSmem {
   static constexpr int K = WS * KS;
   static constexpr int TT = 32 * MT;
   size_t ring, meta, red, srci, st_s, st_lo, st_w, st_sc, bars, misc, total;
-  __host__ __device__ WindowSmem(int rowcap, int max_active) {
+  // row_factor: 32-bit words per ring row per sample of capacity
+  // (ring_row_factor<STORAGE>())
+  __host__ __device__ WindowSmem(int rowcap, int max_active, int row_factor) {
     size_t o = 0;
-    ring = o;        o += (size_t)NSTAGE * P * rowcap * 4;
+    ring = o;        o += (size_t)NSTAGE * P * rowcap * 4 * row_factor;
     o = align_up_sz(o, 16);
     meta = o;        o += (size_t)max_active * K * sizeof(M);
     o = align_up_sz(o, 16);
@@ -316,11 +328,11 @@ struct WindowSmem {
 
 // Sample of accumulator half h of pair q for this lane, relative to t0.
 // FP32: lane owns samples lane + 32 m (pair q = m 2q, 2q+1);
-// 16-bit: lane owns pairs (2 lane + 64 q, 2 lane + 64 q + 1).
+// 16-bit: lane owns runs of 4 samples 4 lane + 128 r (pairs q = 2r, 2r+1).
 template <int STORAGE>
 __device__ __forceinline__ int pair_sample(int lane, int q, int h) {
   if constexpr (STORAGE == BP_STORAGE_F32) return lane + 64 * q + 32 * h;
-  else return 2 * lane + 64 * q + h;
+  else return 4 * lane + 128 * (q >> 1) + 2 * (q & 1) + h;
 }
 
 // The staged shift-and-stack for one item (record, source tile, time tiles
@@ -335,7 +347,9 @@ struct Staged {
   static constexpr int TT = 32 * MT;
   static constexpr int NCONS = WS * 32;
   static constexpr int ESZ = F32 ? 4 : 2;  // bytes per stored element
-  static constexpr int NVER = F32 ? 1 : 2; // stored versions per row
+  static constexpr int NVER = F32 ? 1 : kHalfCopies;  // stored copies per row
+  static constexpr int RF = ring_row_factor<STORAGE>();
+  static_assert(F32 || MT % 4 == 0, "16-bit lanes own runs of 4 samples");
 
   struct Smem {
     unsigned char* ring;
@@ -354,7 +368,7 @@ struct Staged {
   };
 
   __device__ static Smem carve(unsigned char* smem, int rowcap, int max_active) {
-    const WindowSmem<P, KS, MT, WS, NSTAGE, MAXRED> L(rowcap, max_active);
+    const WindowSmem<P, KS, MT, WS, NSTAGE, MAXRED> L(rowcap, max_active, RF);
     Smem s;
     s.ring = smem + L.ring;
     s.meta_s = reinterpret_cast<M*>(smem + L.meta);
@@ -391,7 +405,7 @@ struct Staged {
     const int tid = threadIdx.x;
     const int warp = tid >> 5;
     const int lane = tid & 31;
-    const int row_words = rowcap;  // one ring row (all versions) in 32-bit words
+    const int row_words = rowcap * RF;  // one ring row (all copies) in 32-bit words
 
     // ---- prologue: the tile's stations (those the record uses) ----------
     if (warp == 0) {
@@ -418,18 +432,19 @@ struct Staged {
     const int n_active = *sm.n_act;
     {
       const M* gm = reinterpret_cast<const M*>(tb.meta) + (size_t)tile * tb.S * K;
-      const uint32_t half_row = (uint32_t)rowcap >> 1;
+      const uint32_t copy_words = (uint32_t)rowcap >> 1;  // one 16-bit copy, in words
       for (int i = tid; i < n_active * K; i += blockDim.x) {
         const int jj = i / K, k = i - jj * K;
         M m = gm[(size_t)sm.st_s[jj] * K + k];
         if constexpr (!F32) {
-          // 16-bit: each sample offset becomes the 32-bit word offset in
-          // the ring row, version included: (off >> 1) + (off & 1) * rowcap / 2
-          // (version 1 starts rowcap / 2 words into the row).
+          // 16-bit: each sample offset becomes the (even) 32-bit word offset
+          // in the ring row of the copy that starts the run on an 8-byte
+          // boundary: 2 (off >> 2) + (off & 3) * rowcap / 2 (copy v starts
+          // v * rowcap / 2 words into the row).
           auto wo = [&](uint32_t v) {
             const uint32_t lo = v & 0xFFFFu, hi = v >> 16;
-            return ((lo >> 1) + (lo & 1u) * half_row) |
-                   (((hi >> 1) + (hi & 1u) * half_row) << 16);
+            return (2 * (lo >> 2) + (lo & 3u) * copy_words) |
+                   ((2 * (hi >> 2) + (hi & 3u) * copy_words) << 16);
           };
           m.y = wo(m.y);
           if constexpr (P > 2) m.z = wo(m.z);
@@ -553,16 +568,21 @@ struct Staged {
               // sample pair with c = w * scale (exact: scale is 2^k).
               const float c = w * scale;
               const float2 c2 = make_float2(c, c);
-              const uint32_t* src[P];  // word offsets prepared in the prologue
+              const uint2* src[P];  // word offsets prepared in the prologue (even)
 #pragma unroll
               for (int p = 0; p < P; ++p)
-                src[p] = reinterpret_cast<const uint32_t*>(sm.ring) + sbase + p * row_words +
-                         meta_off<P>(m, p) + lane;
+                src[p] = reinterpret_cast<const uint2*>(
+                             reinterpret_cast<const uint32_t*>(sm.ring) + sbase +
+                             p * row_words + meta_off<P>(m, p)) + lane;
               uint32_t wd[P][MT / 2];  // all words first (see the FP32 path)
 #pragma unroll
               for (int p = 0; p < P; ++p)
 #pragma unroll
-                for (int q = 0; q < MT / 2; ++q) wd[p][q] = src[p][32 * q];
+                for (int r = 0; r < MT / 4; ++r) {
+                  const uint2 v = src[p][32 * r];  // samples 4 lane + 128 r + 0..3
+                  wd[p][2 * r] = v.x;
+                  wd[p][2 * r + 1] = v.y;
+                }
 #pragma unroll
               for (int q = 0; q < MT / 2; ++q) {
                 float2 ps;
@@ -878,7 +898,7 @@ __global__ void __launch_bounds__(256) beam_direct_kernel(const DirectArgs a) {
           const long long tt = t + __ldg(d + s * a.P + p);
           if (tt < 0 || tt >= a.T) continue;
           const size_t row = (STORAGE == BP_STORAGE_F32) ? (size_t)(s * a.P + p)
-                                                         : (size_t)(s * a.P + p) * 2;
+                                                         : (size_t)(s * a.P + p) * kHalfCopies;
           const float u = load_trace<STORAGE>(a.traces, row * a.pitch + a.lpad + tt);
           acc = __fadd_rn(acc, __fmul_rn(w, u));
         }
@@ -1161,7 +1181,7 @@ __global__ void scale_pow2_kernel(unsigned int* __restrict__ scale_bits, int S) 
   reinterpret_cast<float*>(scale_bits)[s] = sc;
 }
 
-// Pass 2: U / scale rounded to 16 bits, both versions, zero padding.
+// Pass 2: U / scale rounded to 16 bits, every shifted copy, zero padding.
 template <int STORAGE>
 __global__ void prestack_h16_kernel(const float* __restrict__ F, const float* __restrict__ alpha,
                                     int T, int S, int C, int P, int lpad, long long pitch,
@@ -1172,7 +1192,7 @@ __global__ void prestack_h16_kernel(const float* __restrict__ F, const float* __
   const int s = blockIdx.y;
   if (r >= pitch) return;
   const float inv = 1.0f / scales[s];  // power of two: exact
-  for (int v = 0; v < 2; ++v) {
+  for (int v = 0; v < kHalfCopies; ++v) {
     const long long t = r - lpad + v;
     const bool in = t >= 0 && t < T;
     for (int p = 0; p < P; ++p) {
@@ -1182,7 +1202,7 @@ __global__ void prestack_h16_kernel(const float* __restrict__ F, const float* __
           acc = __fadd_rn(acc, __fmul_rn(__ldg(alpha + ((size_t)s * C + c) * P + p),
                                          __ldg(F + ((size_t)s * C + c) * T + t)));
       }
-      out[((size_t)(s * P + p) * 2 + v) * pitch + r] = H::from_float(acc * inv);
+      out[((size_t)(s * P + p) * kHalfCopies + v) * pitch + r] = H::from_float(acc * inv);
     }
   }
 }

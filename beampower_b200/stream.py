@@ -27,7 +27,7 @@ import time
 
 import numpy as np
 
-from .core import STORAGE, Record, check, load_library
+from .core import STORAGE, Record, check, load_library, trace_copies
 from .tables import TravelTimeTable, _dev_tensor, _stream_ptr
 
 try:
@@ -74,7 +74,7 @@ class NetworkStream:
     def bytes_per_chunk(self, n_samples):
         """Device bytes one chunk holds while in flight (record + traces + outputs)."""
         rec = n_samples + self.lag - self.lead
-        elem = 4 if self._st == 0 else 4  # 16-bit storage keeps two versions
+        elem = 4 if self._st == 0 else 2 * trace_copies(self._st)  # 16-bit: shifted copies
         return (self.S * self.C * rec * 4 + self.S * self.P * (rec + 1024 + self.lag) * elem
                 + n_samples * 16)
 
@@ -84,7 +84,7 @@ class NetworkStream:
         T = int(record.shape[2])
         lpad, pitch = self.table.layout(T)
         st = self._st
-        rows = self.S * self.P * (1 if st == 0 else 2)
+        rows = self.S * self.P * trace_copies(st)
         elem = torch.float32 if st == 0 else (torch.bfloat16 if st == 1 else torch.float16)
         traces = torch.empty((rows, pitch), dtype=elem, device=self.device)
         scales = torch.ones(self.S, dtype=torch.float32, device=self.device)

@@ -11,7 +11,7 @@ import ctypes as ct
 
 import numpy as np
 
-from .core import STORAGE, TableInfo, check, load_library
+from .core import STORAGE, TableInfo, check, load_library, trace_copies
 
 try:  # torch is plumbing (device memory, streams), imported lazily where needed
     import torch
@@ -103,9 +103,9 @@ class TravelTimeTable:
         st = STORAGE[storage]
         lpad, pitch = self.layout(T)
         elem = torch.float32 if st == 0 else (torch.bfloat16 if st == 1 else torch.float16)
-        # 16-bit storage keeps two versions of every row (the second shifted
-        # by one sample) so that any sample pair is one aligned 32-bit word
-        rows = S * self.n_phases * (1 if st == 0 else 2)
+        # 16-bit storage keeps shifted copies of every row so that any run of
+        # 4 samples is one aligned 64-bit word pair (trace_copies rows per row)
+        rows = S * self.n_phases * trace_copies(st)
         buf = torch.empty((rows, pitch), dtype=elem, device=self.device)
         scales = torch.ones(S, dtype=torch.float32, device=self.device)
         check(self.lib.bp_prestack_dev(F.data_ptr(), A.data_ptr(), T, S, C, self.n_phases, st,
@@ -140,7 +140,7 @@ class TravelTimeTable:
         st = STORAGE[storage]
         lpad, pitch = self.layout(T)
         elem = torch.float32 if st == 0 else (torch.bfloat16 if st == 1 else torch.float16)
-        rows = S * self.n_phases * (1 if st == 0 else 2)
+        rows = S * self.n_phases * trace_copies(st)
         buf = torch.empty((rows, pitch), dtype=elem, device=self.device)
         scales = torch.ones(S, dtype=torch.float32, device=self.device)
         check(self.lib.bp_prestack_envelope_dev(X.data_ptr(), A.data_ptr(), T, S, C,
@@ -205,7 +205,7 @@ class Traces:
 
     def to_prestacked(self, n_phases):
         """Back to the reference's (S, T, P) float32 layout (for checks)."""
-        buf = self.buf if self.storage == 0 else self.buf[0::2]
+        buf = self.buf[0::trace_copies(self.storage)]
         rows = buf[:, self.lpad:self.lpad + self.n_samples].float()
         if self.scales is not None and self.storage != 0:
             rows = rows * self.scales.repeat_interleave(n_phases)[:, None]

@@ -149,9 +149,13 @@ BP_API int bp_table_get_info(const bp_table *table, bp_table_info *info);
 
 /* Layout of device trace storage for a table and a record length: element
  * (s, p, t) sits at row (s * P + p) of `pitch` elements, index lpad + t;
- * indexes outside [lpad, lpad + T) must hold zeros. */
+ * indexes outside [lpad, lpad + T) must hold zeros.  16-bit storage holds
+ * bp_trace_copies(storage) = 4 copies per (s, p): row (s * P + p) * 4 + v,
+ * index lpad + t, holds element t + v (copy v shifted by v samples). */
 BP_API int bp_trace_layout(const bp_table *table, size_t n_samples, size_t *lpad,
                     size_t *pitch);
+/* Rows per (station, phase) of trace storage: 1 for FP32, 4 for BF16 / FP16. */
+BP_API int bp_trace_copies(int storage);
 
 /* Prestack on device: features (S, C, T) f32, weights_phases (S, C, P) f32
  * -> traces in the layout above (element type per `storage`; zero padding is
