@@ -376,6 +376,7 @@ def run_ours(args, rank, world, local_rank):
     info = recs[0][4].info
     # the other trace storage types on the same resident table (kernel only)
     variants = {}
+    run_variants = {}
     if not args.profile:
         vt = recs[-1][4]
         for stg in ("fp32", "fp16", "bf16"):
@@ -394,6 +395,42 @@ def run_ours(args, rank, world, local_rank):
                              "unit": "beam terms/s", "kernel_config":
                              lib.bp_get_kernel_config({"fp32": 0, "bf16": 1, "fp16": 2}[stg], 1)}
             del tr
+        # the other runs of the same configuration: the flexible rule, and
+        # reduce='none' on the first 20,000 sources (a 20,000 x T beam)
+        tr = vt.traces_from_features(dF, dA, storage="fp32")
+        flex = 1 - oob
+        vt.beamform_max(tr, flex)
+        e0, e1 = ev(), ev()
+        e0.record(stream)
+        vt.beamform_max(tr, flex)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        kms = e0.elapsed_time(e1)
+        eff_f = effective_terms(D, W, T, flex == 1)
+        run_variants["flexible" if flex else "strict"] = {
+            "kernel_ms": kms, "value": terms / (kms * 1e-3), "unit": "beam terms/s",
+            "effective_terms": eff_f, "smem_frac": (eff_f * 4 / (kms * 1e-3)) / (smem_gbs.value * 1e9),
+            "storage": "fp32"}
+        del tr
+        n_sub = min(20000, N)
+        sub = TravelTimeTable(dD[:n_sub].contiguous(), dW[:n_sub].contiguous(), device=dev)
+        tr = sub.traces_from_features(dF, dA, storage="fp32")
+        beam = torch.zeros((n_sub, T), dtype=torch.float32, device=dev)
+        sub.beamform(tr, oob, out=beam)
+        e0, e1 = ev(), ev()
+        e0.record(stream)
+        sub.beamform(tr, oob, out=beam)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        kms = e0.elapsed_time(e1)
+        sub_terms = nominal_terms(n_sub, T, S, P)
+        out_bytes = n_sub * T * 4
+        run_variants["reduce_none_20k"] = {
+            "kernel_ms": kms, "value": sub_terms / (kms * 1e-3), "unit": "beam terms/s",
+            "n_sources": n_sub, "output_bytes": out_bytes,
+            "output_gbs": out_bytes / (kms * 1e-3) / 1e9, "storage": "fp32"}
+        del beam, tr
+        sub.close()
     for r in recs:
         r[4].close()
     ms_per_step = elapsed_ms / args.steps
@@ -480,6 +517,7 @@ def run_ours(args, rank, world, local_rank):
             },
             "table": info,
             "storage_variants": variants,
+            "run_variants": run_variants,
             "e2e": {"value": world * terms / e2e_s, "unit": "beam terms/s",
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "seconds_per_step": e2e_s},
