@@ -200,21 +200,25 @@ class StreamScheduler:
             if self.inflight and (self.mem_in_use + need > self.memory_budget or need > free):
                 break  # wait for memory to free up
             self.pending.popleft()
+            admit = time.perf_counter()
             t_emit0 = net.t_emit
+            ev0 = torch.cuda.Event(enable_timing=True)
+            ev0.record(net.stream)
             net.push(chunk)
             terms = (net.t_emit - t_emit0) * net.table.n_sources * net.S * net.P
             ev = torch.cuda.Event(enable_timing=True)
             ev.record(net.stream)
-            self.inflight.append((arrival, name, ev, need, terms))
+            self.inflight.append((arrival, name, ev, need, terms, admit, ev0))
             self.mem_in_use += need
 
     def _retire(self):
         keep = []
         for item in self.inflight:
-            arrival, name, ev, need, terms = item
+            arrival, name, ev, need, terms, admit, ev_start = item
             if ev.query():
                 done_t = self._host0 + self._ev0.elapsed_time(ev) / 1e3
-                self.done.append((name, arrival, done_t, terms))
+                start_t = self._host0 + self._ev0.elapsed_time(ev_start) / 1e3
+                self.done.append((name, arrival, done_t, terms, admit, start_t))
                 self.mem_in_use -= need
             else:
                 keep.append(item)
@@ -231,13 +235,30 @@ class StreamScheduler:
                 time.sleep(1e-4)
 
     def stats(self):
+        """Latency = device completion - arrival, split into the wait before
+        admission (host), admission to the chunk's first device work, and its
+        device time (first to last work of the chunk on its stream)."""
         if not self.done:
             return {}
-        lat = np.array([c - a for _, a, c, _ in self.done])
-        t0 = min(a for _, a, _, _ in self.done)
-        t1 = max(c for _, _, c, _ in self.done)
-        terms = sum(t for *_, t in self.done)
-        return {"chunks": len(self.done), "p50_ms": float(np.percentile(lat, 50) * 1e3),
-                "p99_ms": float(np.percentile(lat, 99) * 1e3),
+        d = self.done
+        lat = np.array([c - a for _, a, c, *_ in d])
+        t0 = min(a for _, a, *_ in d)
+        t1 = max(c for _, _, c, *_ in d)
+        terms = sum(x[3] for x in d)
+        pct = lambda v, q: float(np.percentile(v, q) * 1e3)  # noqa: E731
+        wait = np.array([x[4] - x[1] for x in d])
+        launch = np.array([x[5] - x[4] for x in d])
+        device = np.array([x[2] - x[5] for x in d])
+        per_net = {}
+        for name in sorted({x[0] for x in d}):
+            v = np.array([x[2] - x[1] for x in d if x[0] == name])
+            dv = np.array([x[2] - x[5] for x in d if x[0] == name])
+            per_net[name] = {"chunks": int(v.size), "p50_ms": pct(v, 50), "p99_ms": pct(v, 99),
+                             "device_p50_ms": pct(dv, 50)}
+        return {"chunks": len(d), "p50_ms": pct(lat, 50), "p99_ms": pct(lat, 99),
                 "max_ms": float(lat.max() * 1e3), "terms": terms,
-                "terms_per_s": terms / max(t1 - t0, 1e-9), "span_s": t1 - t0}
+                "terms_per_s": terms / max(t1 - t0, 1e-9), "span_s": t1 - t0,
+                "wait_p50_ms": pct(wait, 50), "wait_p99_ms": pct(wait, 99),
+                "admit_to_start_p50_ms": pct(launch, 50), "admit_to_start_p99_ms": pct(launch, 99),
+                "device_p50_ms": pct(device, 50), "device_p99_ms": pct(device, 99),
+                "per_network": per_net}

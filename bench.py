@@ -61,6 +61,8 @@ def parse():
     ap.add_argument("--windows", type=int, default=128, help="batch workload: windows")
     ap.add_argument("--duration", type=float, default=3.0,
                     help="serving workload: seconds of arrivals")
+    ap.add_argument("--max-inflight", type=int, default=8,
+                    help="serving workload: chunks admitted to the GPU at once")
     ap.add_argument("--rate-scale", type=float, default=1.0,
                     help="serving workload: arrival rate relative to ~200 chunks/s")
     ap.add_argument("--profile", action="store_true",
@@ -678,12 +680,12 @@ def run_serving(args, local_rank):
             arrivals.append((t, n["name"]))
     arrivals.sort()
     # warm-up: one chunk per network
-    sched = StreamScheduler(streams, max_inflight=8, memory_budget=150e9)
+    sched = StreamScheduler(streams, max_inflight=args.max_inflight, memory_budget=150e9)
     for n in nets:
         sched.submit(n["name"], chunks[n["name"]][0])
     sched.drain()
     torch.cuda.synchronize()
-    sched = StreamScheduler(streams, max_inflight=8, memory_budget=150e9)
+    sched = StreamScheduler(streams, max_inflight=args.max_inflight, memory_budget=150e9)
     sampler = ClockSampler(local_rank)
     sampler.start()
     counters = {n["name"]: 1 for n in nets}
@@ -712,9 +714,14 @@ def run_serving(args, local_rank):
         "data": "synthetic",
         "config": {"workload": SERVING.name, "networks": len(nets),
                    "offered_chunks_per_s": offered, "offered_terms_per_s": offered_terms,
-                   "duration_s": args.duration, "max_inflight": 8, "storage": args.storage},
+                   "duration_s": args.duration, "max_inflight": args.max_inflight,
+                   "storage": args.storage},
         "latency_ms": {"p50": st.get("p50_ms"), "p99": st.get("p99_ms"),
                        "max": st.get("max_ms")},
+        "latency_breakdown_ms": {k: st.get(k) for k in (
+            "wait_p50_ms", "wait_p99_ms", "admit_to_start_p50_ms", "admit_to_start_p99_ms",
+            "device_p50_ms", "device_p99_ms")},
+        "per_network": st.get("per_network"),
         "chunks_done": st.get("chunks"), "span_s": st.get("span_s"),
         "clocks": clocks,
     }
