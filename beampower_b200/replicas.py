@@ -1,8 +1,8 @@
 """Multi-GPU runs as independent replicas.
 
-The beamforming hot path has no cross-GPU exchange in this package (the
-north star excludes a multi-GPU split): N processes, one per GPU, each run
-the whole workload.  What is shared is only the measurement: a barrier before
+The beamforming hot path has no cross-GPU exchange in this package (sources
+are independent and the benchmark is quoted on one GPU): N processes, one per
+GPU, each run the whole workload.  What is shared is only the measurement: a barrier before
 and after the timed region, the slowest rank's time (max over ranks), and the
 whole-job rate = N x work / that time.  These helpers work with any
 torch.distributed backend (NCCL on GPUs, gloo on CPU for tests).

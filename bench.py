@@ -16,7 +16,8 @@ the key decode.  Inputs (418 MB) are larger than L2, so no flush is needed.
 ``--impl reference`` times the reference's own C/OpenMP library (compiled
 from its sources into oracle/_ref/) on the host cores, on a bounded
 source sample of the same workload.  Multi-GPU runs are replicas: every rank
-processes the whole workload (the north star has no multi-GPU split).
+processes the whole workload (the benchmark is quoted on one GPU and the path
+has no exchange between GPUs).
 """
 from __future__ import annotations
 
