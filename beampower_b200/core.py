@@ -67,6 +67,23 @@ class Record(ct.Structure):
 
 
 # symbol -> (argtypes, restype)
+class PeakOptions(ct.Structure):
+    """bp_peak_options (include/beampower_b200.h)."""
+
+    _fields_ = [
+        ("distance", ct.c_double),
+        ("use_height", ct.c_int32),
+        ("height_min", ct.c_double),
+        ("height_max", ct.c_double),
+        ("d_height_min", ct.c_void_p),
+        ("d_height_max", ct.c_void_p),
+        ("use_prominence", ct.c_int32),
+        ("prominence_min", ct.c_double),
+        ("prominence_max", ct.c_double),
+        ("wlen", ct.c_double),
+    ]
+
+
 SIGNATURES = {
     # drop-ins, argtypes of beampower/core.py:65-87 (restype added: int status)
     "beamform": ([_f32p, _i32p, _f32p, _sz, _sz, _sz, _sz, _int, _f32p], _int),
@@ -93,6 +110,8 @@ SIGNATURES = {
     "bp_threshold_dev": ([_vp, _sz, _sz, ct.c_double, _int, ct.c_float, _vp, _sz,
                           ct.c_ulonglong, _vp, _vp], _int),
     "bp_find_peaks_dev": ([_vp, _sz, ct.c_double, _vp, _sz, ct.POINTER(_sz), _vp], _int),
+    "bp_find_peaks_opt_dev": ([_vp, _sz, ct.POINTER(PeakOptions), _vp, _vp, _vp, _vp, _sz,
+                               ct.POINTER(_sz), _vp], _int),
     "bp_detect_dev": ([_vp, _vp, _vp, _sz, ct.c_double, _vp, _vp, _vp, _sz, ct.POINTER(_sz),
                        _vp], _int),
     "bp_pairwise_sum_f32": ([_vp, _sz], ct.c_float),

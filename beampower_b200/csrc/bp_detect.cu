@@ -432,13 +432,6 @@ __global__ void kept_flags_kernel(const int* __restrict__ state, int m, int* __r
   flags[j] = (j < m && state[j] == kKept) ? 1 : 0;
 }
 
-__global__ void scatter_peaks_kernel(const int* __restrict__ flags, const int* __restrict__ rank,
-                                     const int* __restrict__ pos, int m, int* __restrict__ out) {
-  const int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= m) return;
-  if (flags[j]) out[rank[j]] = pos[j];
-}
-
 __global__ void above_flags_kernel(const float* __restrict__ x, const float* __restrict__ thr,
                                    const int* __restrict__ peaks, int m, int* __restrict__ flags) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
@@ -464,8 +457,134 @@ __global__ void scatter_detections_kernel(const int* __restrict__ flags,
 
 // ---- host drivers -------------------------------------------------------------
 // Peaks of x into d_peaks (device, ascending); their number into *m_out.
-int find_peaks_impl(const float* x, int n, double distance, int32_t* d_peaks, int* m_out,
-                    Scratch& sc, cudaStream_t st) {
+// ---- height and prominence conditions (SciPy's find_peaks options) ----------
+// lo <= v <= hi in float64; a NaN scalar border is an open side, a per-sample
+// border array (float32, read at the peak) compares as SciPy does (NaN fails).
+__device__ __forceinline__ bool within(double v, double lo, double hi, const float* lo_arr,
+                                       const float* hi_arr, int p) {
+  bool ok = true;
+  if (lo_arr) ok = ok && ((double)lo_arr[p] <= v);
+  else if (!isnan(lo)) ok = ok && (lo <= v);
+  if (hi_arr) ok = ok && (v <= (double)hi_arr[p]);
+  else if (!isnan(hi)) ok = ok && (v <= hi);
+  return ok;
+}
+
+__global__ void height_flags_kernel(const float* __restrict__ x, const int* __restrict__ pos,
+                                    int m, double lo, double hi, const float* __restrict__ lo_arr,
+                                    const float* __restrict__ hi_arr, int* __restrict__ flags) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j > m) return;
+  flags[j] = (j < m && within((double)x[pos[j]], lo, hi, lo_arr, hi_arr, pos[j])) ? 1 : 0;
+}
+
+// One warp per peak: from the peak, walk outwards while the signal is not
+// above it (NaN stops the walk), at most `half` samples when half >= 0; the
+// base of each side is its lowest sample (the one nearest the peak among
+// equals), the prominence the peak minus the higher base, in float64.
+__global__ void prominence_kernel(const float* __restrict__ x, int n, const int* __restrict__ pos,
+                                  int m, long long half, double* __restrict__ prom,
+                                  int* __restrict__ lbase, int* __restrict__ rbase) {
+  const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (gw >= m) return;
+  const int p = pos[gw];
+  const float xp = x[p];
+  const long long lo_end = half >= 0 ? max(0LL, (long long)p - half) : 0LL;
+  const long long hi_end = half >= 0 ? min((long long)n - 1, (long long)p + half)
+                                     : (long long)n - 1;
+  float side_min[2];
+  int side_base[2];
+  for (int dir = 0; dir < 2; ++dir) {  // 0: left, 1: right
+    float best = xp;
+    int best_i = p;
+    for (long long base = p;; base += dir ? 32 : -32) {
+      const long long i = dir ? base + lane : base - lane;
+      const bool inside = dir ? i <= hi_end : i >= lo_end;
+      const float v = inside ? x[i] : 0.0f;
+      const bool walk = inside && v <= xp;  // false past the window, above the peak, NaN
+      const unsigned stop = __ballot_sync(kFull, !walk);
+      const int n_walk = stop ? __ffs(stop) - 1 : 32;  // lanes before the first stop
+      // lowest value among the walked lanes, nearest the peak among equals
+      float cv = lane < n_walk ? v : INFINITY;
+      int ci = lane < n_walk ? (int)i : INT_MAX;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const float ov = __shfl_xor_sync(kFull, cv, o);
+        const int oi = __shfl_xor_sync(kFull, ci, o);
+        const bool nearer = dir ? oi < ci : (oi != INT_MAX && (ci == INT_MAX || oi > ci));
+        if (ov < cv || (ov == cv && nearer)) {
+          cv = ov;
+          ci = oi;
+        }
+      }
+      if (n_walk > 0 && cv < best) {  // a strictly lower sample further out
+        best = cv;
+        best_i = ci;
+      }
+      if (stop) break;
+    }
+    side_min[dir] = best;
+    side_base[dir] = best_i;
+  }
+  if (lane == 0) {
+    prom[gw] = (double)xp - (double)fmaxf(side_min[0], side_min[1]);
+    lbase[gw] = side_base[0];
+    rbase[gw] = side_base[1];
+  }
+}
+
+__global__ void prominence_flags_kernel(const double* __restrict__ prom, int m, double lo,
+                                        double hi, int* __restrict__ flags) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j > m) return;
+  flags[j] = (j < m && within(prom[j], lo, hi, nullptr, nullptr, 0)) ? 1 : 0;
+}
+
+__global__ void compact_peaks_kernel(const int* __restrict__ flags, const int* __restrict__ rank,
+                                     int m, const int* __restrict__ pos,
+                                     const double* __restrict__ prom, const int* __restrict__ lb,
+                                     const int* __restrict__ rb, int* __restrict__ out_pos,
+                                     double* __restrict__ out_prom, int* __restrict__ out_lb,
+                                     int* __restrict__ out_rb) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= m || !flags[j]) return;
+  const int r = rank[j];
+  out_pos[r] = pos[j];
+  if (out_prom) out_prom[r] = prom[j];
+  if (out_lb) out_lb[r] = lb[j];
+  if (out_rb) out_rb[r] = rb[j];
+}
+
+// ---- host driver of the peak finder -----------------------------------------
+struct PeakOut {
+  int32_t* peaks;
+  double* prominences;  // may be NULL
+  int32_t* left_bases;  // may be NULL
+  int32_t* right_bases; // may be NULL
+};
+
+// Keeps the entries of `pos` (m, device) whose flag is set, in order, into a
+// new scratch array; returns their number.
+int keep_flagged(int* flags, int m, int** pos, Scratch& sc, cudaStream_t st, int* kept) {
+  int* rank = nullptr;
+  int* out = nullptr;
+  BP_TRY(sc.get(&rank, (size_t)m + 1));
+  BP_TRY(scan_flags(flags, rank, m, sc, st));
+  BP_TRY(read_back(kept, rank + m, st));
+  BP_TRY(sc.get(&out, std::max(*kept, 1)));
+  compact_peaks_kernel<<<grid_for(m, 256), 256, 0, st>>>(flags, rank, m, *pos, nullptr, nullptr,
+                                                         nullptr, out, nullptr, nullptr,
+                                                         nullptr);
+  BP_LAUNCHED("compact_peaks_kernel");
+  *pos = out;
+  return BP_OK;
+}
+
+// Peaks of x in SciPy's order of conditions: local maxima (plateaus by their
+// midpoint), height, distance, prominence.  Writes `*m_out` entries of `out`.
+int find_peaks_impl(const float* x, int n, const bp_peak_options& o, const PeakOut& out,
+                    int* m_out, Scratch& sc, cudaStream_t st) {
   *m_out = 0;
   if (n < 3) return BP_OK;
   int *flags = nullptr, *rank = nullptr, *plateau = nullptr, *counters = nullptr;
@@ -487,51 +606,88 @@ int find_peaks_impl(const float* x, int n, double distance, int32_t* d_peaks, in
   BP_TRY(scan_flags(flags, rank, n, sc, st));
   int m = 0;
   BP_TRY(read_back(&m, rank + n, st));
-  const bool by_distance = distance > 0.0 && m > 1;
-  int* pos = by_distance ? nullptr : d_peaks;
-  if (by_distance) BP_TRY(sc.get(&pos, m));
+  int* pos = nullptr;
+  BP_TRY(sc.get(&pos, std::max(m, 1)));
   scatter_flagged_kernel<<<grid_for(n, 256), 256, 0, st>>>(flags, rank, n, pos);
   BP_LAUNCHED("scatter_flagged_kernel");
-  if (!by_distance) {
-    *m_out = m;
-    return BP_OK;
+  // height
+  if (o.use_height && m > 0) {
+    height_flags_kernel<<<grid_for((long long)m + 1, 256), 256, 0, st>>>(
+        x, pos, m, o.height_min, o.height_max, o.d_height_min, o.d_height_max, flags);
+    BP_LAUNCHED("height_flags_kernel");
+    BP_TRY(keep_flagged(flags, m, &pos, sc, st, &m));
   }
   // greedy distance rule, in rounds
-  const double dc = std::ceil(distance);
-  const long long dist = dc > (double)n ? (long long)n + 1 : (long long)dc;
-  float* val = nullptr;
-  int *state = nullptr, *und = nullptr, *und2 = nullptr, *kept = nullptr;
-  BP_TRY(sc.get(&val, m));
-  BP_TRY(sc.get(&state, (size_t)m + 1));
-  BP_TRY(sc.get(&und, m));
-  BP_TRY(sc.get(&und2, m));
-  BP_TRY(sc.get(&kept, m));
-  gather_heights_kernel<<<grid_for(m, 256), 256, 0, st>>>(x, pos, m, val, state, und);
-  BP_LAUNCHED("gather_heights_kernel");
-  int u = m;
-  for (int round = 0; u > 0; ++round) {
-    if (round > m) return fail(BP_ERR_KERNEL, "distance rule did not converge");
-    BP_CUDA(cudaMemsetAsync(counters + 1, 0, 2 * sizeof(int), st));
-    const unsigned gw = grid_for((long long)u * 32, 256);
-    distance_keep_kernel<<<gw, 256, 0, st>>>(pos, val, state, m, dist, und, u, kept,
-                                             counters + 1);
-    BP_LAUNCHED("distance_keep_kernel");
-    distance_drop_kernel<<<gw, 256, 0, st>>>(pos, state, m, dist, kept, counters + 1);
-    BP_LAUNCHED("distance_drop_kernel");
-    distance_next_kernel<<<grid_for(u, 256), 256, 0, st>>>(state, und, u, und2, counters + 2);
-    BP_LAUNCHED("distance_next_kernel");
-    BP_TRY(read_back(&u, counters + 2, st));
-    std::swap(und, und2);
+  if (o.distance > 0.0 && m > 1) {
+    const double dc = std::ceil(o.distance);
+    const long long dist = dc > (double)n ? (long long)n + 1 : (long long)dc;
+    float* val = nullptr;
+    int *state = nullptr, *und = nullptr, *und2 = nullptr, *kept = nullptr;
+    BP_TRY(sc.get(&val, m));
+    BP_TRY(sc.get(&state, (size_t)m + 1));
+    BP_TRY(sc.get(&und, m));
+    BP_TRY(sc.get(&und2, m));
+    BP_TRY(sc.get(&kept, m));
+    gather_heights_kernel<<<grid_for(m, 256), 256, 0, st>>>(x, pos, m, val, state, und);
+    BP_LAUNCHED("gather_heights_kernel");
+    int u = m;
+    for (int round = 0; u > 0; ++round) {
+      if (round > m) return fail(BP_ERR_KERNEL, "distance rule did not converge");
+      BP_CUDA(cudaMemsetAsync(counters + 1, 0, 2 * sizeof(int), st));
+      const unsigned gw = grid_for((long long)u * 32, 256);
+      distance_keep_kernel<<<gw, 256, 0, st>>>(pos, val, state, m, dist, und, u, kept,
+                                               counters + 1);
+      BP_LAUNCHED("distance_keep_kernel");
+      distance_drop_kernel<<<gw, 256, 0, st>>>(pos, state, m, dist, kept, counters + 1);
+      BP_LAUNCHED("distance_drop_kernel");
+      distance_next_kernel<<<grid_for(u, 256), 256, 0, st>>>(state, und, u, und2, counters + 2);
+      BP_LAUNCHED("distance_next_kernel");
+      BP_TRY(read_back(&u, counters + 2, st));
+      std::swap(und, und2);
+    }
+    kept_flags_kernel<<<grid_for((long long)m + 1, 256), 256, 0, st>>>(state, m, flags);
+    BP_LAUNCHED("kept_flags_kernel");
+    BP_TRY(keep_flagged(flags, m, &pos, sc, st, &m));
   }
-  kept_flags_kernel<<<grid_for((long long)m + 1, 256), 256, 0, st>>>(state, m, flags);
-  BP_LAUNCHED("kept_flags_kernel");
-  BP_TRY(scan_flags(flags, rank, m, sc, st));
-  int k = 0;
-  BP_TRY(read_back(&k, rank + m, st));
-  scatter_peaks_kernel<<<grid_for(m, 256), 256, 0, st>>>(flags, rank, pos, m, d_peaks);
-  BP_LAUNCHED("scatter_peaks_kernel");
-  *m_out = k;
+  // prominence
+  if (o.use_prominence && m > 0) {
+    double* prom = nullptr;
+    int *lb = nullptr, *rb = nullptr;
+    BP_TRY(sc.get(&prom, m));
+    BP_TRY(sc.get(&lb, m));
+    BP_TRY(sc.get(&rb, m));
+    const long long half = o.wlen > 1.0 ? (long long)std::ceil(o.wlen) / 2 : -1;
+    prominence_kernel<<<grid_for((long long)m * 32, 256), 256, 0, st>>>(x, n, pos, m, half,
+                                                                        prom, lb, rb);
+    BP_LAUNCHED("prominence_kernel");
+    prominence_flags_kernel<<<grid_for((long long)m + 1, 256), 256, 0, st>>>(
+        prom, m, o.prominence_min, o.prominence_max, flags);
+    BP_LAUNCHED("prominence_flags_kernel");
+    int* prank = nullptr;
+    BP_TRY(sc.get(&prank, (size_t)m + 1));
+    BP_TRY(scan_flags(flags, prank, m, sc, st));
+    int k = 0;
+    BP_TRY(read_back(&k, prank + m, st));
+    compact_peaks_kernel<<<grid_for(m, 256), 256, 0, st>>>(flags, prank, m, pos, prom, lb, rb,
+                                                           out.peaks, out.prominences,
+                                                           out.left_bases, out.right_bases);
+    BP_LAUNCHED("compact_peaks_kernel");
+    *m_out = k;
+    return BP_OK;
+  }
+  if (m > 0)
+    BP_CUDA(cudaMemcpyAsync(out.peaks, pos, (size_t)m * sizeof(int32_t),
+                            cudaMemcpyDeviceToDevice, st));
+  *m_out = m;
   return BP_OK;
+}
+
+bp_peak_options distance_only(double distance) {
+  bp_peak_options o{};
+  o.distance = distance;
+  o.height_min = o.height_max = NAN;
+  o.prominence_min = o.prominence_max = NAN;
+  return o;
 }
 
 int check_series(const void* p, size_t n, const char* what) {
@@ -656,7 +812,33 @@ int bp_find_peaks_dev(const float* d_x, size_t n_samples, double distance, int32
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
   Scratch sc(st);
   int m = 0;
-  BP_TRY(find_peaks_impl(d_x, (int)n_samples, distance, d_peaks, &m, sc, st));
+  BP_TRY(find_peaks_impl(d_x, (int)n_samples, distance_only(distance),
+                         PeakOut{d_peaks, nullptr, nullptr, nullptr}, &m, sc, st));
+  BP_CUDA(cudaStreamSynchronize(st));
+  *n_peaks = (size_t)m;
+  return BP_OK;
+}
+
+int bp_find_peaks_opt_dev(const float* d_x, size_t n_samples, const bp_peak_options* opt,
+                          int32_t* d_peaks, double* d_prominences, int32_t* d_left_bases,
+                          int32_t* d_right_bases, size_t capacity, size_t* n_peaks,
+                          void* stream) {
+  BP_TRY(check_series(d_x, n_samples, "series"));
+  if (!n_peaks || !opt) return fail(BP_ERR_INVALID_ARGUMENT, "n_peaks / options is NULL");
+  *n_peaks = 0;
+  if (opt->distance > 0.0 && opt->distance < 1.0)
+    return fail(BP_ERR_INVALID_ARGUMENT, "distance must be greater or equal to 1");
+  if (opt->use_prominence && opt->wlen > 0.0 && std::ceil(opt->wlen) <= 1.0)
+    return fail(BP_ERR_INVALID_ARGUMENT, "wlen must be larger than 1");
+  if (capacity < n_samples / 2 || (!d_peaks && n_samples >= 3))
+    return fail(BP_ERR_INVALID_ARGUMENT, "peak capacity must be at least n_samples / 2");
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  Scratch sc(st);
+  int m = 0;
+  BP_TRY(find_peaks_impl(d_x, (int)n_samples, *opt,
+                         PeakOut{d_peaks, d_prominences, d_left_bases, d_right_bases}, &m, sc,
+                         st));
+  BP_CUDA(cudaStreamSynchronize(st));
   *n_peaks = (size_t)m;
   return BP_OK;
 }
@@ -678,7 +860,8 @@ int bp_detect_dev(const float* d_beam_max, const int32_t* d_argmax, const float*
   int* peaks = nullptr;
   BP_TRY(sc.get(&peaks, n / 2 + 1));
   int m = 0;
-  BP_TRY(find_peaks_impl(d_beam_max, n, distance, peaks, &m, sc, st));
+  BP_TRY(find_peaks_impl(d_beam_max, n, distance_only(distance),
+                         PeakOut{peaks, nullptr, nullptr, nullptr}, &m, sc, st));
   if (m == 0) return BP_OK;
   int *flags = nullptr, *rank = nullptr;
   BP_TRY(sc.get(&flags, (size_t)m + 1));

@@ -14,11 +14,12 @@ Outputs follow the input: numpy in, numpy out; tensor in, tensor out.
 from __future__ import annotations
 
 import ctypes as ct
+import math
 from dataclasses import dataclass
 
 import numpy as np
 
-from .core import check, load_library
+from .core import PeakOptions, check, load_library
 
 try:
     import torch
@@ -86,31 +87,101 @@ def time_dependent_threshold(time_series, sliding_window, overlap=0.66, threshol
     return _out(out, time_series)
 
 
-def find_peaks(x, distance=None):
-    """``(peaks, {})`` as ``scipy.signal.find_peaks(x, distance=distance)``.
+def _borders(interval, n, device):
+    """SciPy's condition argument -> (min, max, min array, max array): a
+    number, a pair, or arrays over the series (read at the peaks)."""
+    try:
+        lo, hi = interval
+    except (TypeError, ValueError):
+        lo, hi = interval, None
+
+    def one(v):
+        if v is None:
+            return float("nan"), None
+        if isinstance(v, np.ndarray) or _is_tensor(v):
+            a = _as_device(v, torch.float32).reshape(-1)
+            if a.numel() != n:
+                raise ValueError("array size of interval border must match x")
+            return float("nan"), a
+        return float(v), None
+
+    (lo_v, lo_a), (hi_v, hi_a) = one(lo), one(hi)
+    return lo_v, hi_v, lo_a, hi_a
+
+
+def find_peaks(x, height=None, threshold=None, distance=None, prominence=None, width=None,
+               wlen=None, rel_height=0.5, plateau_size=None):
+    """``(peaks, properties)`` as ``scipy.signal.find_peaks(x, height=,
+    distance=, prominence=, wlen=)``, with SciPy's parameter order;
+    ``threshold``, ``width`` and ``plateau_size`` are not implemented and
+    raise NotImplementedError when given.
 
     Peaks are the local maxima of x (a flat plateau counts at its midpoint
-    when both its neighbours are lower); with ``distance``, peaks are taken
-    in decreasing height and every peak closer than ``ceil(distance)``
-    samples to a taken one is dropped.  Equal heights: the later sample
-    first (SciPy leaves that order to NumPy's unstable sort).
+    when both its neighbours are lower), then, in SciPy's order: the height
+    condition (a number, a (min, max) pair, or per-sample arrays), the
+    minimum distance (peaks taken in decreasing height; every peak closer
+    than ``ceil(distance)`` samples to a taken one is dropped; equal heights:
+    the later sample first, where SciPy leaves the order to NumPy's unstable
+    sort), and the prominence condition (walks limited to ``wlen``).
+    properties: ``peak_heights`` with height; ``prominences``,
+    ``left_bases``, ``right_bases`` with prominence, as SciPy returns them.
     """
+    for name, v in (("threshold", threshold), ("width", width), ("plateau_size", plateau_size)):
+        if v is not None:
+            raise NotImplementedError(f"find_peaks: `{name}` is not implemented on the GPU")
     lib = load_library("gpu")
     d = _as_device(x, torch.float32)
     if d.ndim != 1:
         raise ValueError("x must be one-dimensional")
     if distance is not None and distance < 1:
         raise ValueError("`distance` must be greater or equal to 1")
+    if wlen is not None and prominence is not None and math.ceil(wlen) <= 1:
+        raise ValueError(f"`wlen` must be larger than 1, was {math.ceil(wlen)}")
     n = int(d.shape[0])
     cap = max(n // 2, 1)
+    opt = PeakOptions()
+    opt.distance = 0.0 if distance is None else float(distance)
+    keep_alive = []
+    if height is not None:
+        opt.use_height = 1
+        opt.height_min, opt.height_max, lo_a, hi_a = _borders(height, n, d.device)
+        keep_alive += [lo_a, hi_a]
+        opt.d_height_min = None if lo_a is None else lo_a.data_ptr()
+        opt.d_height_max = None if hi_a is None else hi_a.data_ptr()
+    else:
+        opt.height_min = opt.height_max = float("nan")
+    if prominence is not None:
+        opt.use_prominence = 1
+        p_lo, p_hi, p_lo_a, p_hi_a = _borders(prominence, n, d.device)
+        if p_lo_a is not None or p_hi_a is not None:
+            raise NotImplementedError("find_peaks: array borders of `prominence`")
+        opt.prominence_min, opt.prominence_max = p_lo, p_hi
+        opt.wlen = 0.0 if wlen is None else float(wlen)
+    else:
+        opt.prominence_min = opt.prominence_max = float("nan")
     peaks = torch.empty(cap, dtype=torch.int32, device=d.device)
+    prom = lb = rb = None
+    if prominence is not None:
+        prom = torch.empty(cap, dtype=torch.float64, device=d.device)
+        lb = torch.empty(cap, dtype=torch.int32, device=d.device)
+        rb = torch.empty(cap, dtype=torch.int32, device=d.device)
     count = ct.c_size_t(0)
     from .tables import _stream_ptr
+    ptr = (lambda t: None if t is None else t.data_ptr())  # noqa: E731
     with torch.cuda.device(d.device):
-        check(lib.bp_find_peaks_dev(d.data_ptr(), n, 0.0 if distance is None else float(distance),
-                                    peaks.data_ptr(), cap, ct.byref(count), _stream_ptr()))
-    p = peaks[:count.value].to(torch.int64)
-    return _out(p, x), {}
+        check(lib.bp_find_peaks_opt_dev(d.data_ptr(), n, ct.byref(opt), peaks.data_ptr(),
+                                        ptr(prom), ptr(lb), ptr(rb), cap, ct.byref(count),
+                                        _stream_ptr()))
+    k = count.value
+    p = peaks[:k].to(torch.int64)
+    props = {}
+    if height is not None:
+        props["peak_heights"] = d[p].to(torch.float64)
+    if prominence is not None:
+        props["prominences"] = prom[:k]
+        props["left_bases"] = lb[:k].to(torch.int64)
+        props["right_bases"] = rb[:k].to(torch.int64)
+    return _out(p, x), {key: _out(v, x) for key, v in props.items()}
 
 
 @dataclass

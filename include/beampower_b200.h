@@ -330,6 +330,31 @@ BP_API int bp_threshold_dev(const float *d_series, size_t n_samples, size_t slid
 BP_API int bp_find_peaks_dev(const float *d_x, size_t n_samples, double distance,
                              int32_t *d_peaks, size_t capacity, size_t *n_peaks, void *stream);
 
+/* SciPy's other find_peaks conditions used around the tutorial (the
+ * prominence / wlen option is shown at notebooks/3_beampower.ipynb:625),
+ * applied in SciPy's order: height, distance, prominence.  Borders are
+ * float64 with NaN for an open side; d_height_min / d_height_max, when not
+ * NULL, give per-sample borders read at the peak (SciPy's array borders). */
+typedef struct bp_peak_options {
+  double distance;          /* <= 0: no distance rule                          */
+  int32_t use_height;       /* 1: keep height_min <= x[peak] <= height_max      */
+  double height_min, height_max;
+  const float *d_height_min, *d_height_max;
+  int32_t use_prominence;   /* 1: keep prominence_min <= prominence <= max      */
+  double prominence_min, prominence_max;
+  double wlen;              /* > 1: prominence walk limited to ceil(wlen) / 2
+                               samples each side; <= 0: whole series            */
+} bp_peak_options;
+
+/* Peaks as scipy.signal.find_peaks(x, height=, distance=, prominence=, wlen=)
+ * (identical indexes; prominences in float64, bases as SciPy's
+ * left_bases / right_bases).  d_prominences / d_left_bases / d_right_bases
+ * may be NULL and are written only with use_prominence.  Synchronises. */
+BP_API int bp_find_peaks_opt_dev(const float *d_x, size_t n_samples, const bp_peak_options *opt,
+                                 int32_t *d_peaks, double *d_prominences,
+                                 int32_t *d_left_bases, int32_t *d_right_bases,
+                                 size_t capacity, size_t *n_peaks, void *stream);
+
 /* Detections (notebooks/3_beampower.ipynb:618-626): the peaks of d_beam_max
  * as above whose height is strictly above d_threshold, with their heights
  * and, when d_argmax is not NULL, the winning source of each. */

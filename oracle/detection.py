@@ -20,9 +20,11 @@ What it restates (file:line in the reference checkout):
 
 SciPy (1.18.1 in this image) is a third-party dependency of the tutorial.  Its
 peak finder is restated here from its published algorithm
-(scipy/signal/_peak_finding_utils.pyx: ``_local_maxima_1d`` and
-``_select_by_peak_distance``), and the tests compare this restatement with
-SciPy itself.  Where SciPy orders equal peak heights through NumPy's
+(scipy/signal/_peak_finding_utils.pyx: ``_local_maxima_1d``,
+``_select_by_peak_distance``, ``_peak_prominences``; scipy/signal/
+_peak_finding.py: the height / prominence conditions), and the tests compare
+this restatement with SciPy itself.  The tutorial uses ``distance`` and shows
+``prominence`` with ``wlen`` as an option (notebooks/3_beampower.ipynb:625).  Where SciPy orders equal peak heights through NumPy's
 (unstable) default argsort, this restatement uses the stable order: among
 equal heights the later sample is considered first.
 """
@@ -131,17 +133,100 @@ def select_by_distance(peaks, priority, distance):
     return keep
 
 
-def find_peaks(x, distance=None):
-    """Sample indexes of the peaks of x, as scipy.signal.find_peaks(x, distance=...)[0]."""
+def interval_borders(interval, x, peaks):
+    """(min, max) borders of a height / prominence condition: a number, a
+    pair, or arrays over x read at the peaks (SciPy's condition arguments)."""
+    try:
+        lo, hi = interval
+    except (TypeError, ValueError):
+        lo, hi = interval, None
+    if isinstance(lo, np.ndarray):
+        if lo.size != x.size:
+            raise ValueError("array size of lower interval border must match x")
+        lo = lo[peaks]
+    if isinstance(hi, np.ndarray):
+        if hi.size != x.size:
+            raise ValueError("array size of upper interval border must match x")
+        hi = hi[peaks]
+    return lo, hi
+
+
+def within(values, lo, hi):
+    keep = np.ones(values.size, dtype=bool)
+    if lo is not None:
+        keep &= lo <= values
+    if hi is not None:
+        keep &= values <= hi
+    return keep
+
+
+def peak_prominences(x, peaks, wlen=None):
+    """(prominences, left_bases, right_bases): from each peak, walk outwards
+    while the signal is not above the peak (at most wlen // 2 samples when
+    wlen is given); the base on each side is the lowest sample met, the
+    prominence the peak minus the higher of the two bases (float64)."""
+    x = np.asarray(x, np.float64)
+    w = -1 if wlen is None else math.ceil(wlen)
+    if wlen is not None and w <= 1:
+        raise ValueError(f"`wlen` must be larger than 1, was {w}")
+    n = x.shape[0]
+    prom = np.empty(len(peaks), np.float64)
+    lb = np.empty(len(peaks), np.int64)
+    rb = np.empty(len(peaks), np.int64)
+    for k, pk in enumerate(peaks):
+        lo_end, hi_end = 0, n - 1
+        if w >= 2:
+            lo_end = max(pk - w // 2, lo_end)
+            hi_end = min(pk + w // 2, hi_end)
+        i = lb[k] = pk
+        left = x[pk]
+        while lo_end <= i and x[i] <= x[pk]:
+            if x[i] < left:
+                left = x[i]
+                lb[k] = i
+            i -= 1
+        i = rb[k] = pk
+        right = x[pk]
+        while i <= hi_end and x[i] <= x[pk]:
+            if x[i] < right:
+                right = x[i]
+                rb[k] = i
+            i += 1
+        prom[k] = x[pk] - max(left, right)
+    return prom, lb, rb
+
+
+def find_peaks(x, distance=None, height=None, prominence=None, wlen=None, properties=False):
+    """Peaks of x as scipy.signal.find_peaks(x, height=, distance=,
+    prominence=, wlen=): local maxima, then the height condition, the
+    distance rule and the prominence condition, in SciPy's order.  Returns
+    the indexes, or (indexes, properties) with ``properties=True``."""
     x = np.asarray(x)
     if x.ndim != 1:
         raise ValueError("x must be one-dimensional")
+    x64 = np.asarray(x, np.float64)
     _l, _r, peaks = local_maxima(x)
+    props = {}
+    if height is not None:
+        h = x64[peaks]
+        lo, hi = interval_borders(height, x64, peaks)
+        keep = within(h, lo, hi)
+        peaks = peaks[keep]
+        props["peak_heights"] = h[keep]
     if distance is not None:
         if distance < 1:
             raise ValueError("distance must be greater or equal to 1")
-        peaks = peaks[select_by_distance(peaks, np.asarray(x, np.float64)[peaks], distance)]
-    return peaks
+        keep = select_by_distance(peaks, x64[peaks], distance)
+        peaks = peaks[keep]
+        props = {k: v[keep] for k, v in props.items()}
+    if prominence is not None:
+        prom, lb, rb = peak_prominences(x64, peaks, wlen)
+        props.update(prominences=prom, left_bases=lb, right_bases=rb)
+        lo, hi = interval_borders(prominence, x64, peaks)
+        keep = within(prom, lo, hi)
+        peaks = peaks[keep]
+        props = {k: v[keep] for k, v in props.items()}
+    return (peaks, props) if properties else peaks
 
 
 def detect(beam_max, threshold, distance):

@@ -84,3 +84,24 @@ def test_pairwise_sum_tree_matches_numpy(bplib):
         got = bplib.bp_pairwise_sum_f32(a.ctypes.data_as(ct.c_void_p), n)
         want = np.sum(a)
         assert np.float32(got).view(np.uint32) == np.float32(want).view(np.uint32), n
+
+
+@pytest.mark.parametrize("seed", [0, 1])
+@pytest.mark.parametrize("kw", [
+    {"height": 0.2}, {"height": (0.1, 0.6)}, {"height": "array"},
+    {"prominence": 0.3}, {"prominence": (0.2, 1.5), "wlen": 25},
+    {"prominence": 0.1, "wlen": 7.5}, {"height": 0.0, "distance": 40, "prominence": 0.25},
+    {"distance": 12, "prominence": (None, 0.8), "wlen": 100}])
+def test_oracle_peak_options_match_scipy(seed, kw):
+    rng = np.random.default_rng(seed)
+    x = np.convolve(rng.standard_normal(4000), np.ones(5) / 5, mode="same").astype(np.float32)
+    x[700:706] = x[700]
+    kw = dict(kw)
+    if kw.get("height") == "array":
+        kw["height"] = (0.1 + 0.2 * np.sin(np.arange(x.size) / 300.0)).astype(np.float32)
+    ref, ref_props = signal.find_peaks(x, **kw)
+    got, props = odet.find_peaks(x, properties=True, **kw)
+    assert np.array_equal(got, ref)
+    assert set(props) == set(ref_props)
+    for k in props:
+        assert np.array_equal(props[k], ref_props[k]), k

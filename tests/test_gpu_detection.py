@@ -129,3 +129,42 @@ def test_edge_cases(cuda):
     x[120], x[121] = 5.0, 5.0
     for dist in (None, 1, 3, 10, 45):
         assert np.array_equal(det.find_peaks(x, distance=dist)[0], odet.find_peaks(x, dist))
+
+
+@pytest.mark.parametrize("seed", [0, 1])
+@pytest.mark.parametrize("kw", [
+    {"height": 0.2}, {"height": (0.1, 0.6)}, {"height": "array"},
+    {"prominence": 0.3}, {"prominence": (0.2, 1.5), "wlen": 25},
+    {"prominence": 0.1, "wlen": 7.5}, {"height": 0.0, "distance": 40, "prominence": 0.25},
+    {"distance": 12, "prominence": (None, 0.8), "wlen": 100}])
+def test_peak_options_match_oracle(cuda, seed, kw):
+    """height / prominence / wlen (the tutorial's commented option at
+    notebooks/3_beampower.ipynb:625): identical peaks and properties."""
+    from oracle import detection as odet
+    rng = np.random.default_rng(seed)
+    x = np.convolve(rng.standard_normal(40000), np.ones(5) / 5, mode="same").astype(np.float32)
+    x[700:706] = x[700]
+    x[9000:9400] = 0.0
+    kw = dict(kw)
+    if kw.get("height") == "array":
+        kw["height"] = (0.1 + 0.2 * np.sin(np.arange(x.size) / 300.0)).astype(np.float32)
+    ref, ref_props = odet.find_peaks(x, properties=True, **kw)
+    got, props = _det().find_peaks(x, **kw)
+    assert np.array_equal(got, ref)
+    assert set(props) == set(ref_props)
+    for k in props:
+        assert np.array_equal(props[k], ref_props[k]), k
+
+
+def test_prominence_without_window_on_a_day(cuda):
+    """Prominence walks with no window over a day-long series (the highest
+    peaks walk to the series ends), against SciPy itself (the oracle's walk
+    in Python would take minutes here; it is checked against SciPy on the
+    CPU)."""
+    from scipy import signal
+    x = _day_series(14, 2_160_000, 2864)
+    ref, ref_props = signal.find_peaks(x, distance=1500, prominence=20.0)
+    got, props = _det().find_peaks(x, distance=1500, prominence=20.0)
+    assert ref.size > 10 and np.array_equal(got, ref)
+    for k in ("prominences", "left_bases", "right_bases"):
+        assert np.array_equal(props[k], ref_props[k]), k
