@@ -116,6 +116,8 @@ SIGNATURES = {
                        _vp], _int),
     "bp_pairwise_sum_f32": ([_vp, _sz], ct.c_float),
     "bp_trace_copies": ([_int], _int),
+    "bp_keys_to_shared_dev": ([_vp, _sz, _sz, _vp], _int),
+    "bp_keys_from_shared_dev": ([_vp, _sz, _vp, _vp, _vp], _int),
     "bp_envelope_dev": ([_vp, _sz, _sz, ct.c_float, _vp, _vp], _int),
     "bp_seconds_to_samples_dev": ([_vp, _sz, _sz, ct.c_double, ct.c_double, _int, _vp, _vp],
                                   _int),

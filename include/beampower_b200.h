@@ -407,6 +407,20 @@ BP_API int bp_seconds_to_samples_dev(const float *d_seconds, size_t n_sources,
  * GPU.  No reference counterpart. */
 BP_API float bp_pairwise_sum_f32(const float *x, size_t n);
 
+/* ---- sources split over GPUs ---------------------------------------------
+ * The reference splits sources over the visible GPUs and merges the partial
+ * maxima on the host (beampower/src/beamform.cu:227-276, 430-445).  Here each
+ * rank runs bp_beamform_max_dev on its block of sources (a table of those
+ * sources) and keeps the keys buffer; bp_keys_to_shared_dev rebases the keys
+ * to global source indexes (source_offset = the block's first source) and
+ * maps them to signed order, an elementwise int64 max all-reduce over the
+ * ranks merges them (NCCL, torch.distributed), and bp_keys_from_shared_dev
+ * decodes the merged keys.  Results equal the single-GPU call bit for bit. */
+BP_API int bp_keys_to_shared_dev(unsigned long long *d_keys, size_t n_samples,
+                                 size_t source_offset, void *stream);
+BP_API int bp_keys_from_shared_dev(const unsigned long long *d_keys, size_t n_samples,
+                                   float *d_beam_max, int32_t *d_argmax, void *stream);
+
 /* ---- staged-kernel configurations (autotuning) -------------------------- */
 /* The staged kernel exists in several shapes (sources per thread, samples per
  * lane, consumer warps, ring stages), all over the same 64-source tables.
