@@ -10,6 +10,12 @@ tutorial to float32 FFT rounding.
 
 ``TravelTimeTable.traces_from_waveforms`` goes one step further: raw
 waveforms straight to the beamformer's trace rows.
+
+Inputs are converted to float32 first.  The tutorial's traces may be
+float64 (as ObsPy reads them), in which case SciPy computes their envelope in
+float64 before the float32 feature array stores it; the float32 FFTs here
+then differ from it by float32 rounding, within the same bound as from the
+float32 tutorial path.
 """
 from __future__ import annotations
 

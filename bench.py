@@ -861,9 +861,42 @@ def run_stages(args, local_rank):
                          "seconds": cpu_ing, "sample": "the whole grid (NumPy)"}}
     # ---- the tutorial end to end (4,000 sources x 20 stations x 6,000 samples) ----
     out["pipeline"] = _pipeline_stage(dev, gpu_ms)
+    out["pipeline_large"] = _pipeline_large(dev)
     clocks = sampler.stop()
     print(json.dumps({"workload": "stages", "n_gpus": 1, "steps": steps, "warmup": warm,
                       "data": "synthetic", "stages": out, "clocks": clocks}), flush=True)
+
+
+def _pipeline_large(dev):
+    """The tutorial end to end at the scale of the 400,000-source network:
+    raw waveforms (60 x 3 x 180,000) and travel times in seconds
+    (400,000 x 60 x 2) to detections, one call; GPU time only (the CPU
+    reference's beamforming alone would take about ten minutes here, see the
+    main benchmark's cpu_baseline)."""
+    import torch
+    from beampower_b200.pipeline import detect_events
+    wl = make_workload(LARGE)
+    fs = LARGE.fs
+    D, W, A = wl["time_delays"], wl["weights_sources"], wl["weights_phases"]
+    rng = np.random.default_rng(9)
+    F = wl["waveform_features"]
+    raw = torch.from_numpy((rng.standard_normal(F.shape) * (1.0 + F)).astype(np.float32)).to(dev)
+    tt = torch.from_numpy((D / fs).astype(np.float32)).to(dev)
+    kw = dict(window_duration_sec=600.0, num_dev=8.0, min_detection_interval_sec=60.0)
+    detect_events(raw, tt, fs, A, W, **kw)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    ev = detect_events(raw, tt, fs, A, W, **kw)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    N, S, P = D.shape
+    return {"workload": LARGE.name + ", raw waveforms + travel times (s) -> detections",
+            "ms": ms, "detections": int(ev.peaks.numel()),
+            "beam_terms_per_s": nominal_terms(N, F.shape[2], S, P) / (ms * 1e-3),
+            "note": "one call: travel-time conversion, table build, envelope features, "
+                    "prestack, beamform_max, threshold, detections"}
 
 
 def _pipeline_stage(dev, gpu_ms):
