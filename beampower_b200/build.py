@@ -85,6 +85,11 @@ def build(force: bool = False, verbose: bool = False, extra=(), jobs=None) -> st
     from concurrent.futures import ThreadPoolExecutor
     with ThreadPoolExecutor(max_workers=jobs) as ex:
         results = list(ex.map(compile_one, sources()))
+    # objects of sources that no longer exist
+    current = {obj for _s, obj, _r in results}
+    for stale in glob.glob(os.path.join(objdir, "*.o")):
+        if stale not in current:
+            os.remove(stale)
     failed = False
     for src, _obj, r in results:
         if r.stdout or r.stderr:
