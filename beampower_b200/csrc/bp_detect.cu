@@ -18,6 +18,9 @@
 //    undecided peak within the distance of a kept one is dropped.
 #define BP_TEMPLATE_KERNELS_ONLY
 #include <cmath>
+#include <map>
+#include <mutex>
+#include <utility>
 
 #include "bp_stats.cuh"
 
@@ -161,31 +164,97 @@ __global__ void pw_inner_kernel(const int4* __restrict__ inner, const int* __res
 
 // out[w] = mean (mode 0) or population variance (mode 1, given the means) of
 // segments of `len` values starting every seg_stride values.
+// Split trees of the lengths seen so far, built and uploaded once per device
+// and kept for the life of the process (up to kTreeCache lengths; beyond
+// that a tree is uploaded into the call's scratch).  The upload is
+// synchronous, so a cached tree is complete before any stream uses it.
+struct DevTree {
+  int n_leaves = 0, n_inner = 0, n_levels = 0, n_nodes = 0, root = 0;
+  const int4* leaves = nullptr;
+  const int4* inner = nullptr;
+  const int* levels = nullptr;
+};
+constexpr size_t kTreeCache = 64;
+std::mutex g_tree_mu;
+std::map<std::pair<int, int>, DevTree> g_trees;
+
+int upload_tree(const PwTree& t, DevTree* d, void* mem) {
+  char* p = static_cast<char*>(mem);
+  d->n_leaves = (int)t.leaves.size();
+  d->n_inner = (int)t.inner.size();
+  d->n_levels = (int)t.level_end.size();
+  d->n_nodes = t.n_nodes;
+  d->root = t.root;
+  d->leaves = reinterpret_cast<const int4*>(p);
+  d->inner = reinterpret_cast<const int4*>(p + t.leaves.size() * sizeof(int4));
+  d->levels = reinterpret_cast<const int*>(p + (t.leaves.size() + t.inner.size()) *
+                                                   sizeof(int4));
+  BP_CUDA(cudaMemcpy(p, t.leaves.data(), t.leaves.size() * sizeof(int4),
+                     cudaMemcpyHostToDevice));
+  if (!t.inner.empty()) {
+    BP_CUDA(cudaMemcpy(p + t.leaves.size() * sizeof(int4), t.inner.data(),
+                       t.inner.size() * sizeof(int4), cudaMemcpyHostToDevice));
+    BP_CUDA(cudaMemcpy(p + (t.leaves.size() + t.inner.size()) * sizeof(int4),
+                       t.level_end.data(), t.level_end.size() * sizeof(int),
+                       cudaMemcpyHostToDevice));
+  }
+  return BP_OK;
+}
+
+size_t tree_bytes(const PwTree& t) {
+  return (t.leaves.size() + t.inner.size()) * sizeof(int4) + t.level_end.size() * sizeof(int) +
+         16;
+}
+
+int get_tree(int len, DevTree* out, Scratch& sc) {
+  int dev = 0;
+  BP_CUDA(cudaGetDevice(&dev));
+  const auto key = std::make_pair(dev, len);
+  {
+    std::lock_guard<std::mutex> lock(g_tree_mu);
+    auto it = g_trees.find(key);
+    if (it != g_trees.end()) {
+      *out = it->second;
+      return BP_OK;
+    }
+  }
+  const PwTree t = pw_tree(len);
+  std::lock_guard<std::mutex> lock(g_tree_mu);
+  auto it = g_trees.find(key);
+  if (it != g_trees.end()) {
+    *out = it->second;
+    return BP_OK;
+  }
+  void* mem = nullptr;
+  if (g_trees.size() < kTreeCache) {
+    BP_CUDA(cudaMalloc(&mem, tree_bytes(t)));
+    DevTree d;
+    if (int rc = upload_tree(t, &d, mem)) {
+      cudaFree(mem);
+      return rc;
+    }
+    g_trees.emplace(key, d);
+    *out = d;
+    return BP_OK;
+  }
+  char* scratch = nullptr;  // cache full: this call's own copy
+  BP_TRY(sc.get(&scratch, tree_bytes(t)));
+  BP_CUDA(cudaStreamSynchronize(sc.st));  // the scratch is stream-ordered
+  return upload_tree(t, out, scratch);
+}
+
 int pw_mean(const float* x, long long seg_stride, int len, int n_seg, int mode,
             const float* centre, float* out, Scratch& sc, cudaStream_t st) {
-  const PwTree t = pw_tree(len);
-  int4 *d_leaves = nullptr, *d_inner = nullptr;
-  int* d_levels = nullptr;
+  DevTree t;
+  BP_TRY(get_tree(len, &t, sc));
   float* vals = nullptr;
-  BP_TRY(sc.get(&d_leaves, t.leaves.size()));
-  BP_TRY(sc.get(&d_inner, t.inner.size()));
-  BP_TRY(sc.get(&d_levels, t.level_end.size()));
   BP_TRY(sc.get(&vals, (size_t)t.n_nodes * n_seg));
-  BP_CUDA(cudaMemcpyAsync(d_leaves, t.leaves.data(), t.leaves.size() * sizeof(int4),
-                          cudaMemcpyHostToDevice, st));
-  if (!t.inner.empty()) {
-    BP_CUDA(cudaMemcpyAsync(d_inner, t.inner.data(), t.inner.size() * sizeof(int4),
-                            cudaMemcpyHostToDevice, st));
-    BP_CUDA(cudaMemcpyAsync(d_levels, t.level_end.data(), t.level_end.size() * sizeof(int),
-                            cudaMemcpyHostToDevice, st));
-  }
-  const int nl = (int)t.leaves.size();
-  dim3 g1((nl + 127) / 128, (unsigned)std::min(n_seg, 65535));
-  pw_leaves_kernel<<<g1, 128, 0, st>>>(x, seg_stride, mode, centre, d_leaves, nl, t.n_nodes,
-                                       n_seg, vals);
+  dim3 g1((t.n_leaves + 127) / 128, (unsigned)std::min(n_seg, 65535));
+  pw_leaves_kernel<<<g1, 128, 0, st>>>(x, seg_stride, mode, centre, t.leaves, t.n_leaves,
+                                       t.n_nodes, n_seg, vals);
   BP_LAUNCHED("pw_leaves_kernel");
   pw_inner_kernel<<<(unsigned)std::min(n_seg, 65535), n_seg == 1 ? 1024 : 256, 0, st>>>(
-      d_inner, d_levels, (int)t.level_end.size(), t.n_nodes, t.root, len, n_seg, vals, out);
+      t.inner, t.levels, t.n_levels, t.n_nodes, t.root, len, n_seg, vals, out);
   BP_LAUNCHED("pw_inner_kernel");
   return BP_OK;
 }

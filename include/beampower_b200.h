@@ -300,7 +300,9 @@ BP_API int bp_beamform_differential_dev(const float *d_traces, size_t n_samples,
  * results (float32 arithmetic in NumPy's own order, SciPy's peak rules).
  * Each allocates its scratch with cudaMallocAsync on `stream` and
  * synchronises `stream` (it reads counts back), so none of them can be
- * captured in a CUDA graph. */
+ * captured in a CUDA graph.  bp_threshold_dev keeps the pairwise-sum split
+ * tree of each length it has seen on the device (cudaMalloc, up to 64 lengths
+ * per process, freed at exit). */
 
 #define BP_THRESHOLD_RMS 0 /* window mean + num_dev * standard deviation */
 #define BP_THRESHOLD_MAD 1 /* window median + num_dev * median |x - median| */
