@@ -125,3 +125,35 @@ def test_precision_report(cuda, orc, capsys):
     with capsys.disabled():
         for row in report:
             print("PRECISION " + json.dumps(row))
+
+
+@pytest.mark.parametrize("storage", ["fp16", "bf16"])
+def test_16bit_nan_in_weighted_trace(cuda, orc, storage):
+    """A NaN in a weighted station's trace: as in the FP32 path (and the
+    reference), a NaN beam is never the maximum; samples whose every
+    candidate beam is NaN keep 0 / argmax 0; the rest agree with float64
+    within the storage tolerance, argmax identical above the margin."""
+    import beampower_b200 as bp
+    rng = np.random.default_rng(12)
+    S, C, P, T, N = 4, 2, 2, 600, 64
+    F = np.abs(rng.standard_normal((S, C, T))).astype(np.float32)
+    A = rng.uniform(0.0, 1.5, size=(S, C, P)).astype(np.float32)
+    D = rng.integers(0, 51, size=(N, S, P)).astype(np.int32)
+    W = rng.uniform(0.25, 2.0, size=(N, S)).astype(np.float32)
+    F[1, 0, 200:210] = np.nan
+    tol = TOL[storage]
+    beam64, valid = orc.fp64_beams(orc.fp64_prestack(F, A), D, W, 0)
+    finite = valid & np.isfinite(beam64)
+    bm, am = bp.beamform(F, D, A, W, reduce="max", storage=storage)
+    bm32, am32 = bp.beamform(F, D, A, W, reduce="max", storage="fp32")
+    none = ~finite.any(axis=0)
+    assert np.array_equal(bm[none], bm32[none]) and np.all(am[none] == 0) and none.any()
+    b = np.where(finite, beam64, -np.inf)
+    order = np.argsort(-b, axis=0)
+    top1 = np.take_along_axis(b, order[:1], axis=0)[0]
+    top2 = np.take_along_axis(b, order[1:2], axis=0)[0]
+    has = ~none
+    rel = np.abs(bm[has] - top1[has]) / np.abs(top1[has])
+    assert rel.max() <= tol
+    sure = has & ((top1 - top2) > tol * np.abs(top1))
+    assert np.array_equal(am[sure], order[0][sure])
