@@ -513,6 +513,7 @@ uint64_t bp_launch_count(void) { return g_launches.load(); }
 // ---------------------------------------------------------------------------
 int bp_table_create(const int32_t* d_delays, const float* d_weights, size_t N, size_t S,
                     size_t P, void* stream, bp_table** out) {
+  BP_NVTX("bp_table_create");
   g_last_error.clear();
   if (!out) return fail(BP_ERR_INVALID_ARGUMENT, "out_table is NULL");
   *out = nullptr;
@@ -697,6 +698,7 @@ int bp_minmax_dev(const int32_t* d, const float* w, size_t N, size_t S, size_t P
 int bp_prestack_dev(const float* F, const float* alpha, size_t T, size_t S, size_t C, size_t P,
                     int storage, size_t lpad, size_t pitch, void* traces, float* scales,
                     void* stream) {
+  BP_NVTX("bp_prestack_dev");
   g_last_error.clear();
   if (int rc = check_sizes(T, 0, S, P)) return rc;
   if (C == 0 || C > 65535) return fail(BP_ERR_INVALID_ARGUMENT, "bad n_channels %zu", C);
@@ -751,6 +753,7 @@ int bp_beamform_max_dev(const bp_table* t, const void* traces, int storage, cons
                         size_t T, size_t lpad, size_t pitch, int out_of_bounds,
                         unsigned long long* keys, float* beam_max, int32_t* argmax,
                         void* stream) {
+  BP_NVTX("bp_beamform_max_dev");
   g_last_error.clear();
   if (!t) return fail(BP_ERR_INVALID_ARGUMENT, "NULL table");
   if (out_of_bounds != 0 && out_of_bounds != 1)
@@ -783,6 +786,7 @@ int bp_beamform_max_dev(const bp_table* t, const void* traces, int storage, cons
 int bp_beamform_dev(const bp_table* t, const void* traces, int storage, const float* scales,
                     size_t T, size_t lpad, size_t pitch, int out_of_bounds, float* beam,
                     size_t ldb, void* stream) {
+  BP_NVTX("bp_beamform_dev");
   g_last_error.clear();
   if (!t) return fail(BP_ERR_INVALID_ARGUMENT, "NULL table");
   if (out_of_bounds != 0 && out_of_bounds != 1)
@@ -807,6 +811,7 @@ int bp_beamform_max_direct_dev(const void* traces, int storage, const float* sca
                                const float* weights, size_t N, size_t S, size_t P,
                                int out_of_bounds, unsigned long long* keys, float* beam_max,
                                int32_t* argmax, void* stream) {
+  BP_NVTX("bp_beamform_max_direct_dev");
   g_last_error.clear();
   if (int rc = check_sizes(T, N, S, P)) return rc;
   if (out_of_bounds != 0 && out_of_bounds != 1)
@@ -930,6 +935,7 @@ extern "C" {
 int beamform(float* waveform_features, int* time_delays, float* weights, size_t n_samples,
              size_t n_sources, size_t n_stations, size_t n_phases, int out_of_bounds,
              float* beam) {
+  BP_NVTX("beamform");
   return prestacked_entry(waveform_features, time_delays, weights, n_samples, n_sources,
                           n_stations, n_phases, out_of_bounds, BP_REDUCE_NONE, nullptr, nullptr,
                           beam);
@@ -938,6 +944,7 @@ int beamform(float* waveform_features, int* time_delays, float* weights, size_t 
 int beamform_max(float* waveform_features, int* time_delays, float* weights, size_t n_samples,
                  size_t n_sources, size_t n_stations, size_t n_phases, int out_of_bounds,
                  float* beam_max, int* source_index_beam_max) {
+  BP_NVTX("beamform_max");
   return prestacked_entry(waveform_features, time_delays, weights, n_samples, n_sources,
                           n_stations, n_phases, out_of_bounds, BP_REDUCE_MAX, beam_max,
                           source_index_beam_max, nullptr);
@@ -945,6 +952,7 @@ int beamform_max(float* waveform_features, int* time_delays, float* weights, siz
 
 int prestack_waveform_features(float* F, float* alpha, size_t T, size_t S, size_t C, size_t P,
                                int num_threads, float* out) {
+  BP_NVTX("prestack_waveform_features");
   (void)num_threads;
   g_last_error.clear();
   if (int rc = check_sizes(T, 0, S, P)) return rc;
@@ -974,6 +982,7 @@ int prestack_waveform_features(float* F, float* alpha, size_t T, size_t S, size_
 int bp_beamform_host(const float* F, const float* alpha, const int32_t* delays, const float* w,
                      size_t T, size_t N, size_t S, size_t C, size_t P, int oob, int reduce,
                      int storage, float* beam_max, int32_t* argmax, float* beam) {
+  BP_NVTX("bp_beamform_host");
   g_last_error.clear();
   if (int rc = check_sizes(T, N, S, P)) return rc;
   if (C == 0 || C > 65535) return fail(BP_ERR_INVALID_ARGUMENT, "bad n_channels %zu", C);
@@ -1019,6 +1028,7 @@ extern "C" {
 int bp_beamform_differential_dev(const float* traces, size_t T, size_t lpad, size_t pitch,
                                  const int32_t* delays, const float* weights, size_t N, size_t S,
                                  size_t P, float* beam, void* stream) {
+  BP_NVTX("bp_beamform_differential_dev");
   g_last_error.clear();
   if (int rc = check_sizes(T, N, S, P)) return rc;
   if (N == 0 || T == 0) return BP_OK;
@@ -1032,6 +1042,7 @@ int bp_beamform_differential_dev(const float* traces, size_t T, size_t lpad, siz
 
 int beamform_differential(float* U, int* delays, float* w, size_t T, size_t N, size_t S,
                           size_t P, int num_threads, float* beam) {
+  BP_NVTX("beamform_differential");
   (void)num_threads;
   g_last_error.clear();
   if (int rc = check_sizes(T, N, S, P)) return rc;
@@ -1248,6 +1259,7 @@ int bp_batch_create(const bp_table* const* tables, int n_tables, const bp_record
 }
 
 int bp_batch_run(bp_batch* b, void* stream) {
+  BP_NVTX("bp_batch_run");
   g_last_error.clear();
   if (!b) return fail(BP_ERR_INVALID_ARGUMENT, "NULL batch");
   cudaStream_t st = as_stream(stream);
@@ -1293,6 +1305,7 @@ extern "C" {
 
 int bp_record_beamform_max_dev(const bp_table* t, const bp_record* q, int storage,
                                unsigned long long* keys, void* stream) {
+  BP_NVTX("bp_record_beamform_max_dev");
   g_last_error.clear();
   if (!t || !q || !keys) return fail(BP_ERR_INVALID_ARGUMENT, "NULL argument");
   if (!t->info.uses_window_kernel)

@@ -785,6 +785,7 @@ int bp_threshold_dev(const float* d_series, size_t n_samples, size_t sliding_win
                      double overlap, int kind, float num_dev, const float* d_white_noise,
                      size_t n_white_noise, unsigned long long seed, float* d_threshold,
                      void* stream) {
+  BP_NVTX("bp_threshold_dev");
   BP_TRY(check_series(d_series, n_samples, "series"));
   if (!d_threshold) return fail(BP_ERR_INVALID_ARGUMENT, "threshold output is NULL");
   if (kind != BP_THRESHOLD_RMS && kind != BP_THRESHOLD_MAD)
@@ -871,6 +872,7 @@ int bp_threshold_dev(const float* d_series, size_t n_samples, size_t sliding_win
 
 int bp_find_peaks_dev(const float* d_x, size_t n_samples, double distance, int32_t* d_peaks,
                       size_t capacity, size_t* n_peaks, void* stream) {
+  BP_NVTX("bp_find_peaks_dev");
   BP_TRY(check_series(d_x, n_samples, "series"));
   if (!n_peaks) return fail(BP_ERR_INVALID_ARGUMENT, "n_peaks is NULL");
   *n_peaks = 0;
@@ -892,6 +894,7 @@ int bp_find_peaks_opt_dev(const float* d_x, size_t n_samples, const bp_peak_opti
                           int32_t* d_peaks, double* d_prominences, int32_t* d_left_bases,
                           int32_t* d_right_bases, size_t capacity, size_t* n_peaks,
                           void* stream) {
+  BP_NVTX("bp_find_peaks_opt_dev");
   BP_TRY(check_series(d_x, n_samples, "series"));
   if (!n_peaks || !opt) return fail(BP_ERR_INVALID_ARGUMENT, "n_peaks / options is NULL");
   *n_peaks = 0;
@@ -915,6 +918,7 @@ int bp_find_peaks_opt_dev(const float* d_x, size_t n_samples, const bp_peak_opti
 int bp_detect_dev(const float* d_beam_max, const int32_t* d_argmax, const float* d_threshold,
                   size_t n_samples, double distance, int32_t* d_peaks, float* d_heights,
                   int32_t* d_sources, size_t capacity, size_t* n_detections, void* stream) {
+  BP_NVTX("bp_detect_dev");
   BP_TRY(check_series(d_beam_max, n_samples, "beam_max"));
   BP_TRY(check_series(d_threshold, n_samples, "threshold"));
   if (!n_detections) return fail(BP_ERR_INVALID_ARGUMENT, "n_detections is NULL");

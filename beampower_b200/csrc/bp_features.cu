@@ -196,6 +196,7 @@ extern "C" {
 
 int bp_envelope_dev(const float* d_x, size_t n_rows, size_t n_samples, float clip_max,
                     float* d_out, void* stream) {
+  BP_NVTX("bp_envelope_dev");
   if (n_rows == 0 || n_samples == 0) return BP_OK;
   if (!d_x || !d_out) return fail(BP_ERR_INVALID_ARGUMENT, "NULL pointer");
   if (n_samples > (size_t)INT_MAX / 2)
@@ -212,6 +213,7 @@ int bp_prestack_envelope_dev(const float* d_waveforms, const float* d_weights_ph
                              size_t n_samples, size_t n_stations, size_t n_channels,
                              size_t n_phases, float clip_max, int storage, size_t lpad,
                              size_t pitch, void* d_traces, float* d_scales, void* stream) {
+  BP_NVTX("bp_prestack_envelope_dev");
   if (n_samples == 0 || n_stations == 0 || n_channels == 0) return BP_OK;
   if (!d_waveforms || !d_weights_phases || !d_traces)
     return fail(BP_ERR_INVALID_ARGUMENT, "NULL pointer");

@@ -11,6 +11,7 @@
 #include <limits>
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include "beampower_b200.h"
 #include "bp_kernels.cuh"
@@ -23,6 +24,15 @@ int fail(int code, const char* fmt, ...);
 int cuda_fail(cudaError_t e, const char* what);
 // Kernels launched by the library (bp_launch_count()).
 extern std::atomic<uint64_t> g_launches;
+
+// A named range over a public entry point, for timeline profilers (NVTX v3:
+// header only; it costs a check when no tool is attached).
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 int device_sm_count(int dev);
 int device_smem_optin(int dev);
@@ -78,6 +88,8 @@ extern template int launch_window_c<1, false>(int, bool, int, const bp::LaunchAr
     cudaError_t e_ = (call);                                       \
     if (e_ != cudaSuccess) return ::bp_host::cuda_fail(e_, #call); \
   } while (0)
+
+#define BP_NVTX(name) ::bp_host::NvtxRange bp_nvtx_range_(name)
 
 #define BP_LAUNCHED(what)                                                  \
   do {                                                                     \

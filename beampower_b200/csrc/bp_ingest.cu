@@ -59,6 +59,7 @@ extern "C" int bp_seconds_to_samples_dev(const float* d_seconds, size_t n_source
                                          size_t n_per_source, double sampling_rate,
                                          double epsilon, int relative, int32_t* d_delays,
                                          void* stream) {
+  BP_NVTX("bp_seconds_to_samples_dev");
   const size_t n = n_sources * n_per_source;
   if (n == 0) return BP_OK;
   if (!d_seconds || !d_delays) return fail(BP_ERR_INVALID_ARGUMENT, "NULL pointer");

@@ -56,6 +56,7 @@ extern "C" {
 
 int bp_keys_to_shared_dev(unsigned long long* d_keys, size_t n, size_t source_offset,
                           void* stream) {
+  BP_NVTX("bp_keys_to_shared_dev");
   if (n == 0) return BP_OK;
   if (!d_keys) return fail(BP_ERR_INVALID_ARGUMENT, "NULL keys");
   if (source_offset > 0x7FFFFFFFull)
@@ -69,6 +70,7 @@ int bp_keys_to_shared_dev(unsigned long long* d_keys, size_t n, size_t source_of
 
 int bp_keys_from_shared_dev(const unsigned long long* d_keys, size_t n, float* d_beam_max,
                             int32_t* d_argmax, void* stream) {
+  BP_NVTX("bp_keys_from_shared_dev");
   if (n == 0) return BP_OK;
   if (!d_keys || !d_beam_max || !d_argmax) return fail(BP_ERR_INVALID_ARGUMENT, "NULL pointer");
   keys_from_shared_kernel<<<(unsigned)((n + 255) / 256), 256, 0,

@@ -10,6 +10,9 @@ offline call would use is available, so the emitted beams are the offline
 beams, bit for bit with FP32 storage (strict and flexible rules alike).  The
 carried part is the features from (next g to emit) + min(0, min_delay) on.
 ``flush()`` ends the record and emits the rest with the record's true length.
+``state()`` / ``restore()`` (and ``save`` / ``load`` to a file) checkpoint that
+carried halo and the stream position, so a stream can resume in another
+process and still give the offline results.
 
 ``StreamScheduler`` is the request loop over many networks (continuous
 batching): chunks are queued on arrival and admitted while fewer than
@@ -152,6 +155,51 @@ class NetworkStream:
                 self.results.append(out)
                 self.t_emit = self.t_end
         return out
+
+    # ---- checkpoint / resume ------------------------------------------------
+    def state(self):
+        """Host snapshot of what the stream carries between chunks: the
+        not-yet-emitted features (the max-delay halo) and the stream position.
+        Results already emitted are the caller's (``collect``) and are not in
+        the snapshot.  Synchronises the stream."""
+        self.stream.synchronize()
+        info = self.table.info
+        return {"carry": self.carry.cpu().numpy(), "t_end": self.t_end,
+                "t_emit": self.t_emit, "lead": self.lead, "lag": self.lag,
+                "n_sources": self.table.n_sources, "n_stations": self.S,
+                "n_channels": self.C, "n_phases": self.P,
+                "min_delay": info["min_delay"], "max_delay": info["max_delay"]}
+
+    def restore(self, state):
+        """Continue from a snapshot taken by ``state()`` (this object's table
+        and weights must be the snapshot's network): later chunks give the
+        results the uninterrupted stream would have given."""
+        info = self.table.info
+        for key, mine in (("n_sources", self.table.n_sources), ("n_stations", self.S),
+                          ("n_channels", self.C), ("n_phases", self.P),
+                          ("min_delay", info["min_delay"]), ("max_delay", info["max_delay"]),
+                          ("lead", self.lead), ("lag", self.lag)):
+            if int(state[key]) != int(mine):
+                raise ValueError(f"snapshot of another network: {key} {state[key]} != {mine}")
+        carry = np.asarray(state["carry"], dtype=np.float32)
+        if carry.shape != (self.S, self.C, int(state["t_end"]) - int(state["t_emit"])
+                           - self.lead):
+            raise ValueError("snapshot carry does not match its stream position")
+        with torch.cuda.stream(self.stream):
+            self.carry = torch.from_numpy(np.ascontiguousarray(carry)).to(self.device)
+        self.t_end = int(state["t_end"])
+        self.t_emit = int(state["t_emit"])
+        self.results = []
+        return self
+
+    def save(self, path):
+        """``state()`` written to an .npz file."""
+        np.savez(path, **{k: np.asarray(v) for k, v in self.state().items()})
+
+    def load(self, path):
+        """``restore()`` from a file written by ``save()``."""
+        with np.load(path) as z:
+            return self.restore({k: z[k] for k in z.files})
 
     def collect(self):
         """All emitted results as numpy arrays (synchronises the stream)."""

@@ -87,3 +87,45 @@ def test_scheduler_mix_equals_alone(cuda):
         assert np.array_equal(am, alone[k][1]), k
     st = sched.stats()
     assert st["chunks"] == 2 * len(CHUNKS) and st["p99_ms"] >= st["p50_ms"] >= 0
+
+
+@pytest.mark.parametrize("oob,dlo", [("strict", 0), ("flexible", -90)])
+@pytest.mark.parametrize("cut", [1, 3, 5])
+def test_checkpoint_and_resume_equals_offline(cuda, oracle_lib, tmp_path, oob, dlo, cut):
+    """Stream the first `cut` chunks, save the stream's state to a file,
+    resume it in a fresh NetworkStream (new table object, as another process
+    would build it), stream the rest: the two parts together equal one
+    offline call bit for bit."""
+    from beampower_b200.stream import NetworkStream
+    from beampower_b200.tables import TravelTimeTable
+    A, D, W, F = _net(30 + cut + abs(dlo), dlo=dlo)
+    first = NetworkStream(TravelTimeTable(D, W), A, out_of_bounds=oob)
+    t = 0
+    for L in CHUNKS[:cut]:
+        first.push(F[:, :, t:t + L])
+        t += L
+    bm1, am1 = first.collect()
+    path = tmp_path / "stream_state.npz"
+    first.save(path)
+    second = NetworkStream(TravelTimeTable(D, W), A, out_of_bounds=oob).load(path)
+    for L in CHUNKS[cut:]:
+        second.push(F[:, :, t:t + L])
+        t += L
+    second.flush()
+    bm2, am2 = second.collect()
+    bm, am = np.concatenate([bm1, bm2]), np.concatenate([am1, am2])
+    obm, oam = oracle_lib.beamform_max(oracle_lib.prestack(F, A), D, W,
+                                       0 if oob == "strict" else 1)
+    assert np.array_equal(bits(bm), bits(obm)) and np.array_equal(am, oam)
+
+
+def test_restore_rejects_another_network(cuda):
+    from beampower_b200.stream import NetworkStream
+    from beampower_b200.tables import TravelTimeTable
+    A, D, W, F = _net(41)
+    a = NetworkStream(TravelTimeTable(D, W), A)
+    a.push(F[:, :, :700])
+    st = a.state()
+    A2, D2, W2, _ = _net(42, N=500)
+    with pytest.raises(ValueError):
+        NetworkStream(TravelTimeTable(D2, W2), A2).restore(st)
