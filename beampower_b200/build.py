@@ -2,6 +2,7 @@
 
     python -m beampower_b200.build            # build if sources changed
     python -m beampower_b200.build --force    # always rebuild
+    python -m beampower_b200.build --checked  # the index-checked variant
 """
 from __future__ import annotations
 
@@ -16,6 +17,9 @@ CSRC = os.path.join(PKG, "csrc")
 INCLUDE = os.path.join(ROOT, "include")
 LIBDIR = os.path.join(PKG, "lib")
 LIB = os.path.join(LIBDIR, "libbeampower_b200.so")
+# The same sources with the staged kernel's index checks compiled in
+# (BP_DEBUG_CHECKS): load it with BEAMPOWER_B200_LIBRARY=<path>.
+CHECKED_LIB = os.path.join(LIBDIR, "libbeampower_b200_checked.so")
 
 COMPILE_FLAGS = [
     "-O3",
@@ -43,10 +47,10 @@ def _deps():
             glob.glob(os.path.join(INCLUDE, "*.h")) + [os.path.abspath(__file__)])
 
 
-def up_to_date() -> bool:
-    if not os.path.exists(LIB):
+def up_to_date(lib=LIB) -> bool:
+    if not os.path.exists(lib):
         return False
-    t = os.path.getmtime(LIB)
+    t = os.path.getmtime(lib)
     return all(os.path.getmtime(p) <= t for p in _deps())
 
 
@@ -62,13 +66,18 @@ def _host_compiler():
     return ["-ccbin", "/usr/bin/g++"] if os.path.exists("/usr/bin/gcc") else []
 
 
-def build(force: bool = False, verbose: bool = False, extra=(), jobs=None) -> str:
+def build(force: bool = False, verbose: bool = False, extra=(), jobs=None,
+          checked: bool = False) -> str:
     """Compile every .cu under csrc/ (one nvcc per file, in parallel) and link
-    them into one shared library; return its path."""
-    if not force and up_to_date():
-        return LIB
+    them into one shared library; return its path.  checked=True builds the
+    index-checked variant (CHECKED_LIB) from the same sources."""
+    lib = CHECKED_LIB if checked else LIB
+    if checked:
+        extra = (*extra, "-DBP_DEBUG_CHECKS=1")
+    if not force and up_to_date(lib):
+        return lib
     os.makedirs(LIBDIR, exist_ok=True)
-    objdir = os.path.join(LIBDIR, "obj")
+    objdir = os.path.join(LIBDIR, "obj_checked" if checked else "obj")
     os.makedirs(objdir, exist_ok=True)
     cc = _host_compiler()
     jobs = jobs or max(1, min(len(sources()), os.cpu_count() or 1))
@@ -100,7 +109,7 @@ def build(force: bool = False, verbose: bool = False, extra=(), jobs=None) -> st
             sys.stderr.write(f"nvcc failed on {src}\n")
     if failed:
         raise subprocess.CalledProcessError(1, "nvcc")
-    tmp = LIB + ".tmp"
+    tmp = lib + ".tmp"
     # cuFFT (envelope features) is found through the toolkit's lib64 at run time
     cuda_lib = os.path.join(os.path.dirname(os.path.dirname(os.path.realpath(
         nvcc() if os.path.sep in nvcc() else "/usr/local/cuda/bin/nvcc"))), "lib64")
@@ -109,11 +118,12 @@ def build(force: bool = False, verbose: bool = False, extra=(), jobs=None) -> st
     if verbose:
         print(" ".join(cmd), flush=True)
     subprocess.run(cmd, check=True)
-    os.replace(tmp, LIB)
-    return LIB
+    os.replace(tmp, lib)
+    return lib
 
 
 if __name__ == "__main__":
     args = sys.argv[1:]
     ptxas = ["-Xptxas", "-v"] if "--ptxas-v" in args else []
-    print(build(force="--force" in args or bool(ptxas), verbose=True, extra=ptxas))
+    print(build(force="--force" in args or bool(ptxas), verbose=True, extra=ptxas,
+                checked="--checked" in args))

@@ -190,7 +190,9 @@ def load_library(device: str = "gpu"):
     info = LIBRARIES[device_name]
     if info["is_loaded"]:
         return info["lib"]
-    path = info["filepath_library"]
+    # BEAMPOWER_B200_LIBRARY selects another build of the library, e.g. the
+    # index-checked one (lib/libbeampower_b200_checked.so)
+    path = os.environ.get("BEAMPOWER_B200_LIBRARY") or info["filepath_library"]
     if not os.path.exists(path):
         raise RuntimeError(
             f"GPU library not available. The shared object {path} does not exist.\n"

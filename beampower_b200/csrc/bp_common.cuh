@@ -69,6 +69,7 @@ __host__ __device__ __forceinline__ float key_value(unsigned long long key) {
 enum : int {
   kStatusWaitTimeout = 1,   // an mbarrier wait gave up after its time limit
   kStatusBadWindow = 2,     // a trace window did not fit the shared-memory row
+  kStatusBadIndex = 4,      // checked build: an index check failed, the access was skipped
 };
 
 // Wall-clock limit of one mbarrier wait.  A stage normally lands within

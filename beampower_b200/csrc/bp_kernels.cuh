@@ -32,6 +32,14 @@ constexpr int kAlign = 8;
 // by v samples, so that any run of 4 samples is one 8-byte-aligned pair of
 // 32-bit words in one of the copies (one 64-bit shared load per lane).
 constexpr int kHalfCopies = 4;
+// Checked build (-DBP_DEBUG_CHECKS=1, libbeampower_b200_checked.so): the
+// staged kernel checks every bulk copy against the trace buffer and its ring
+// row and every shared-memory read against the copied window; a failed check
+// records kStatusBadIndex in the status word and skips the access (a skipped
+// copy is left out of the stage's expected bytes, so no wait depends on it).
+#ifndef BP_DEBUG_CHECKS
+#define BP_DEBUG_CHECKS 0
+#endif
 // 32-bit words of one ring row per sample of window capacity: FP32 1, 16-bit
 // 2 (kHalfCopies copies of 2-byte elements).
 template <int STORAGE>
@@ -496,13 +504,27 @@ struct Staged {
           const int j = r - (r / n_active) * n_active;
           const int t0 = tau * TT;
           const int s = sm.st_s[j];
+          // copy (p, v) reads trace row (s P + p) NVER + v, columns [col, col + w)
+          auto copy_ok = [&](int p) -> bool {
+#if BP_DEBUG_CHECKS
+            const int w = min(sm.st_w[j * P + p], rowcap);
+            const long long col = (long long)rc.lpad + t0 + sm.st_lo[j * P + p];
+            return s >= 0 && s < tb.S && w > 0 && col >= 0 && col + w <= rc.pitch &&
+                   (col * ESZ) % 16 == 0 && ((long long)w * ESZ) % 16 == 0;
+#else
+            (void)p;
+            return true;
+#endif
+          };
           uint32_t bytes = 0;
 #pragma unroll
           for (int p = 0; p < P; ++p)
-            bytes += (uint32_t)min(sm.st_w[j * P + p], rowcap) * ESZ * NVER;
+            if (copy_ok(p)) bytes += (uint32_t)min(sm.st_w[j * P + p], rowcap) * ESZ * NVER;
+            else atomicOr(status, kStatusBadIndex);
           mbar_arrive_expect_tx(&sm.full[stage], bytes);
 #pragma unroll
           for (int p = 0; p < P; ++p) {
+            if (!copy_ok(p)) continue;
             const int w = min(sm.st_w[j * P + p], rowcap);
             const long long col = (long long)rc.lpad + t0 + sm.st_lo[j * P + p];
 #pragma unroll
@@ -579,6 +601,18 @@ struct Staged {
               for (int p = 0; p < P; ++p)
 #pragma unroll
                 for (int r = 0; r < MT / 4; ++r) {
+#if BP_DEBUG_CHECKS
+                  {  // the 4 samples of this load inside its copy's window
+                    const int copy_words = rowcap >> 1;
+                    const int wi = meta_off<P>(m, p) + 2 * lane + 64 * r;
+                    const int cv = wi / copy_words, pos = 2 * (wi - cv * copy_words);
+                    if (cv >= NVER || pos + 3 >= min(sm.st_w[j * P + p], rowcap)) {
+                      atomicOr(status, kStatusBadIndex);
+                      wd[p][2 * r] = wd[p][2 * r + 1] = 0u;
+                      continue;
+                    }
+                  }
+#endif
                   const uint2 v = src[p][32 * r];  // samples 4 lane + 128 r + 0..3
                   wd[p][2 * r] = v.x;
                   wd[p][2 * r + 1] = v.y;
@@ -616,6 +650,12 @@ struct Staged {
                 for (int mm = 0; mm < MT; ++mm) {
                   const long long tt = tb0 + 32 * mm;
                   if (tt < 0 || tt >= rc.T) continue;
+#if BP_DEBUG_CHECKS
+                  if (off + lane + 32 * mm >= min(sm.st_w[j * P + p], rowcap)) {
+                    atomicOr(status, kStatusBadIndex);
+                    continue;
+                  }
+#endif
                   const float v = __fadd_rn((mm & 1) ? acc[k][mm >> 1].y : acc[k][mm >> 1].x,
                                             __fmul_rn(w, src[mm * 32]));
                   if (mm & 1) acc[k][mm >> 1].y = v; else acc[k][mm >> 1].x = v;
@@ -631,7 +671,16 @@ struct Staged {
               for (int p = 0; p < P; ++p) {
                 const float* src = sbf + p * row_words + meta_off<P>(m, p);
 #pragma unroll
-                for (int mm = 0; mm < MT; ++mm) u[p][mm] = src[32 * mm];
+                for (int mm = 0; mm < MT; ++mm) {
+#if BP_DEBUG_CHECKS
+                  if (meta_off<P>(m, p) + lane + 32 * mm >= min(sm.st_w[j * P + p], rowcap)) {
+                    atomicOr(status, kStatusBadIndex);
+                    u[p][mm] = 0.0f;
+                    continue;
+                  }
+#endif
+                  u[p][mm] = src[32 * mm];
+                }
               }
               if (w == 1.0f) {  // warp-uniform: 1 * u == u exactly, skip the multiply
 #pragma unroll
