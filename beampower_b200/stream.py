@@ -217,12 +217,22 @@ class StreamScheduler:
     networks: dict name -> NetworkStream
     max_inflight: chunks admitted to the GPU at once
     memory_budget: device bytes the in-flight chunks may hold
+    max_wait: seconds a chunk may wait for admission (None: no limit).  A
+        chunk that waited longer ends its network's stream: skipping one
+        chunk would break the carried halo, so that chunk and the network's
+        later pending chunks are dropped (``timed_out``) and the network
+        takes no more chunks.  ``cancel(name)`` ends a stream the same way on
+        request; chunks already on the GPU complete.
     """
 
-    def __init__(self, networks, max_inflight=8, memory_budget=150e9):
+    def __init__(self, networks, max_inflight=8, memory_budget=150e9, max_wait=None):
         self.networks = dict(networks)
         self.max_inflight = max_inflight
         self.memory_budget = memory_budget
+        self.max_wait = max_wait
+        self.closed = {}  # name -> "cancelled" or "timed out"
+        self.cancelled = []  # (name, arrival) of chunks dropped by cancel()
+        self.timed_out = []  # (name, arrival) of chunks dropped by max_wait
         self.pending = collections.deque()  # (arrival, name, chunk)
         self.inflight = []  # (arrival, name, event, bytes, terms)
         self.mem_in_use = 0
@@ -237,11 +247,36 @@ class StreamScheduler:
         self._host0 = time.perf_counter()
 
     def submit(self, name, chunk, arrival=None):
+        if name not in self.networks:
+            raise KeyError(f"unknown network {name!r}")
+        if name in self.closed:
+            raise ValueError(f"network {name!r} takes no more chunks ({self.closed[name]})")
         self.pending.append((time.perf_counter() if arrival is None else arrival, name, chunk))
+
+    def _drop(self, name, reason, into):
+        """End network `name`'s stream: its pending chunks leave the queue."""
+        self.closed[name] = reason
+        keep = collections.deque()
+        for item in self.pending:
+            if item[1] == name:
+                into.append((name, item[0]))
+            else:
+                keep.append(item)
+        self.pending = keep
+
+    def cancel(self, name):
+        """Stop network `name`: drop its chunks not yet admitted (returns how
+        many); chunks already on the GPU complete."""
+        before = len(self.cancelled)
+        self._drop(name, "cancelled", self.cancelled)
+        return len(self.cancelled) - before
 
     def _admit(self):
         while self.pending and len(self.inflight) < self.max_inflight:
             arrival, name, chunk = self.pending[0]
+            if self.max_wait is not None and time.perf_counter() - arrival > self.max_wait:
+                self._drop(name, "timed out", self.timed_out)
+                continue
             net = self.networks[name]
             need = net.bytes_per_chunk(int(chunk.shape[2]))
             free, _ = torch.cuda.mem_get_info(self.device)

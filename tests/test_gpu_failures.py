@@ -72,3 +72,56 @@ def test_scheduler_respects_memory_budget(cuda):
         sched.step()
         peak = max(peak, len(sched.inflight))
     assert peak == 1 and len(sched.done) == 6
+
+
+def _two_networks(rng):
+    from beampower_b200.stream import NetworkStream
+    from beampower_b200.tables import TravelTimeTable
+    S, C, P, N = 6, 3, 2, 300
+    nets, data = {}, {}
+    for name in ("a", "b"):
+        A = rng.uniform(0.2, 1.2, size=(S, C, P)).astype(np.float32)
+        D = rng.integers(0, 80, size=(N, S, P)).astype(np.int32)
+        W = np.ones((N, S), np.float32)
+        nets[name] = NetworkStream(TravelTimeTable(D, W), A)
+        data[name] = (A, D, W, np.abs(rng.standard_normal((S, C, 1500))).astype(np.float32))
+    return nets, data
+
+
+def test_cancelled_stream(cuda, oracle_lib):
+    """Cancelling network b drops its queued chunks and refuses new ones;
+    network a streams on and still equals its offline call."""
+    from beampower_b200.stream import StreamScheduler
+    nets, data = _two_networks(np.random.default_rng(2))
+    sched = StreamScheduler(nets, max_inflight=2)
+    for i in range(3):
+        for name in ("a", "b"):
+            sched.submit(name, data[name][3][:, :, i * 500:(i + 1) * 500])
+    assert sched.cancel("b") == 3
+    with pytest.raises(ValueError):
+        sched.submit("b", data["b"][3][:, :, :500])
+    sched.drain()
+    assert [x[0] for x in sched.done] == ["a"] * 3 and len(sched.cancelled) == 3
+    nets["a"].flush()
+    bm, am = nets["a"].collect()
+    A, D, W, F = data["a"]
+    obm, oam = oracle_lib.beamform_max(oracle_lib.prestack(F, A), D, W, 0)
+    assert np.array_equal(bm.view(np.uint32), obm.view(np.uint32)) and np.array_equal(am, oam)
+
+
+def test_queue_timeout_ends_that_stream(cuda):
+    """A chunk that waited past max_wait ends its network's stream (its later
+    queued chunks are dropped with it); the other network is served."""
+    import time
+    from beampower_b200.stream import StreamScheduler
+    nets, data = _two_networks(np.random.default_rng(3))
+    sched = StreamScheduler(nets, max_inflight=2, max_wait=1.0)
+    now = time.perf_counter()
+    for i in range(2):
+        sched.submit("b", data["b"][3][:, :, i * 500:(i + 1) * 500], arrival=now - 10.0)
+        sched.submit("a", data["a"][3][:, :, i * 500:(i + 1) * 500])
+    sched.drain()
+    assert len(sched.timed_out) == 2 and sched.closed == {"b": "timed out"}
+    assert [x[0] for x in sched.done] == ["a", "a"]
+    with pytest.raises(ValueError):
+        sched.submit("b", data["b"][3][:, :, :500])
