@@ -231,6 +231,9 @@ class StreamScheduler:
         self.memory_budget = memory_budget
         self.max_wait = max_wait
         self.closed = {}  # name -> "cancelled" or "timed out"
+        self.peak_pending = 0  # deepest queue seen
+        self.peak_inflight = 0
+        self.peak_mem = 0  # most device bytes admitted at once
         self.cancelled = []  # (name, arrival) of chunks dropped by cancel()
         self.timed_out = []  # (name, arrival) of chunks dropped by max_wait
         self.pending = collections.deque()  # (arrival, name, chunk)
@@ -308,8 +311,11 @@ class StreamScheduler:
         self.inflight = keep
 
     def step(self):
+        self.peak_pending = max(self.peak_pending, len(self.pending))
         self._retire()
         self._admit()
+        self.peak_inflight = max(self.peak_inflight, len(self.inflight))
+        self.peak_mem = max(self.peak_mem, self.mem_in_use)
 
     def drain(self):
         while self.pending or self.inflight:
@@ -344,4 +350,7 @@ class StreamScheduler:
                 "wait_p50_ms": pct(wait, 50), "wait_p99_ms": pct(wait, 99),
                 "admit_to_start_p50_ms": pct(launch, 50), "admit_to_start_p99_ms": pct(launch, 99),
                 "device_p50_ms": pct(device, 50), "device_p99_ms": pct(device, 99),
+                "peak_queue_depth": self.peak_pending, "peak_inflight": self.peak_inflight,
+                "peak_device_bytes_admitted": self.peak_mem,
+                "cancelled": len(self.cancelled), "timed_out": len(self.timed_out),
                 "per_network": per_net}

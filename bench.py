@@ -732,6 +732,8 @@ def run_serving(args, local_rank):
         "latency_breakdown_ms": {k: st.get(k) for k in (
             "wait_p50_ms", "wait_p99_ms", "admit_to_start_p50_ms", "admit_to_start_p99_ms",
             "device_p50_ms", "device_p99_ms")},
+        "queue": {k: st.get(k) for k in ("peak_queue_depth", "peak_inflight",
+                                          "peak_device_bytes_admitted")},
         "per_network": st.get("per_network"),
         "chunks_done": st.get("chunks"), "span_s": st.get("span_s"),
         "clocks": clocks,

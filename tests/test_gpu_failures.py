@@ -72,6 +72,9 @@ def test_scheduler_respects_memory_budget(cuda):
         sched.step()
         peak = max(peak, len(sched.inflight))
     assert peak == 1 and len(sched.done) == 6
+    st = sched.stats()
+    assert st["peak_inflight"] == 1 and st["peak_queue_depth"] >= 5
+    assert 0 < st["peak_device_bytes_admitted"] <= budget
 
 
 def _two_networks(rng):
