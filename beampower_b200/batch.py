@@ -23,7 +23,7 @@ from dataclasses import dataclass
 import numpy as np
 
 from .core import STORAGE, Record, check, load_library, trace_copies
-from .tables import TravelTimeTable, _dev_tensor, _stream_ptr
+from .tables import _dev_tensor, _stream_ptr
 
 try:
     import torch

@@ -169,7 +169,7 @@ def _cpu_sample(wl, n_sub):
 def time_reference_cpu(wl, oob, target_s, threads):
     """Reference prestack + beamform_max on a source sample sized for about
     target_s seconds.  Returns (terms/s, seconds, sources in sample)."""
-    from oracle.oracle import Reference, REF_CPU_SO, Oracle
+    from oracle.oracle import Reference, Oracle
     kind = "reference"
     try:
         impl = Reference()

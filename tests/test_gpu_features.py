@@ -14,7 +14,6 @@ the seismic-like traces, 5e5 for the spike trace, whose MAD is at the FFT
 rounding level of the spike (there the check is mostly that the clip at 1e5
 holds).
 """
-import os
 
 import numpy as np
 import pytest
