@@ -77,9 +77,16 @@ class PeakOptions(ct.Structure):
         ("height_max", ct.c_double),
         ("d_height_min", ct.c_void_p),
         ("d_height_max", ct.c_void_p),
+        ("use_threshold", ct.c_int32),
+        ("threshold_min", ct.c_double),
+        ("threshold_max", ct.c_double),
+        ("d_threshold_min", ct.c_void_p),
+        ("d_threshold_max", ct.c_void_p),
         ("use_prominence", ct.c_int32),
         ("prominence_min", ct.c_double),
         ("prominence_max", ct.c_double),
+        ("d_prominence_min", ct.c_void_p),
+        ("d_prominence_max", ct.c_void_p),
         ("wlen", ct.c_double),
     ]
 

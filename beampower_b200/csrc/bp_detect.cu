@@ -527,24 +527,50 @@ __global__ void scatter_detections_kernel(const int* __restrict__ flags,
 // ---- host drivers -------------------------------------------------------------
 // Peaks of x into d_peaks (device, ascending); their number into *m_out.
 // ---- height and prominence conditions (SciPy's find_peaks options) ----------
-// lo <= v <= hi in float64; a NaN scalar border is an open side, a per-sample
-// border array (float32, read at the peak) compares as SciPy does (NaN fails).
-__device__ __forceinline__ bool within(double v, double lo, double hi, const float* lo_arr,
-                                       const float* hi_arr, int p) {
+// lo <= v_lo and v_hi <= hi in float64; a NaN scalar border is an open side,
+// a per-sample border array (float64, read at the peak) compares as SciPy
+// does (NaN fails).
+__device__ __forceinline__ bool within(double v_lo, double v_hi, double lo, double hi,
+                                       const double* lo_arr, const double* hi_arr, int p) {
   bool ok = true;
-  if (lo_arr) ok = ok && ((double)lo_arr[p] <= v);
-  else if (!isnan(lo)) ok = ok && (lo <= v);
-  if (hi_arr) ok = ok && (v <= (double)hi_arr[p]);
-  else if (!isnan(hi)) ok = ok && (v <= hi);
+  if (lo_arr) ok = ok && (lo_arr[p] <= v_lo);
+  else if (!isnan(lo)) ok = ok && (lo <= v_lo);
+  if (hi_arr) ok = ok && (v_hi <= hi_arr[p]);
+  else if (!isnan(hi)) ok = ok && (v_hi <= hi);
   return ok;
 }
 
-__global__ void height_flags_kernel(const float* __restrict__ x, const int* __restrict__ pos,
-                                    int m, double lo, double hi, const float* __restrict__ lo_arr,
-                                    const float* __restrict__ hi_arr, int* __restrict__ flags) {
+// SciPy's threshold condition: the peak's rise over each neighbour (float64),
+// the smaller rise against the lower border, the larger against the upper.
+// A peak's neighbours exist and are never NaN (both are below the peak).
+__global__ void threshold_flags_kernel(const float* __restrict__ x, const int* __restrict__ pos,
+                                       int m, double lo, double hi,
+                                       const double* __restrict__ lo_arr,
+                                       const double* __restrict__ hi_arr,
+                                       int* __restrict__ flags) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j > m) return;
-  flags[j] = (j < m && within((double)x[pos[j]], lo, hi, lo_arr, hi_arr, pos[j])) ? 1 : 0;
+  int keep = 0;
+  if (j < m) {
+    const int p = pos[j];
+    const double left = (double)x[p] - (double)x[p - 1];
+    const double right = (double)x[p] - (double)x[p + 1];
+    keep = within(fmin(left, right), fmax(left, right), lo, hi, lo_arr, hi_arr, p) ? 1 : 0;
+  }
+  flags[j] = keep;
+}
+
+__global__ void height_flags_kernel(const float* __restrict__ x, const int* __restrict__ pos,
+                                    int m, double lo, double hi, const double* __restrict__ lo_arr,
+                                    const double* __restrict__ hi_arr, int* __restrict__ flags) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j > m) return;
+  int keep = 0;
+  if (j < m) {
+    const double v = (double)x[pos[j]];
+    keep = within(v, v, lo, hi, lo_arr, hi_arr, pos[j]) ? 1 : 0;
+  }
+  flags[j] = keep;
 }
 
 // One warp per peak: from the peak, walk outwards while the signal is not
@@ -603,11 +629,14 @@ __global__ void prominence_kernel(const float* __restrict__ x, int n, const int*
   }
 }
 
-__global__ void prominence_flags_kernel(const double* __restrict__ prom, int m, double lo,
-                                        double hi, int* __restrict__ flags) {
+__global__ void prominence_flags_kernel(const double* __restrict__ prom,
+                                        const int* __restrict__ pos, int m, double lo, double hi,
+                                        const double* __restrict__ lo_arr,
+                                        const double* __restrict__ hi_arr,
+                                        int* __restrict__ flags) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j > m) return;
-  flags[j] = (j < m && within(prom[j], lo, hi, nullptr, nullptr, 0)) ? 1 : 0;
+  flags[j] = (j < m && within(prom[j], prom[j], lo, hi, lo_arr, hi_arr, pos[j])) ? 1 : 0;
 }
 
 __global__ void compact_peaks_kernel(const int* __restrict__ flags, const int* __restrict__ rank,
@@ -686,6 +715,14 @@ int find_peaks_impl(const float* x, int n, const bp_peak_options& o, const PeakO
     BP_LAUNCHED("height_flags_kernel");
     BP_TRY(keep_flagged(flags, m, &pos, sc, st, &m));
   }
+  // threshold
+  if (o.use_threshold && m > 0) {
+    threshold_flags_kernel<<<grid_for((long long)m + 1, 256), 256, 0, st>>>(
+        x, pos, m, o.threshold_min, o.threshold_max, o.d_threshold_min, o.d_threshold_max,
+        flags);
+    BP_LAUNCHED("threshold_flags_kernel");
+    BP_TRY(keep_flagged(flags, m, &pos, sc, st, &m));
+  }
   // greedy distance rule, in rounds
   if (o.distance > 0.0 && m > 1) {
     const double dc = std::ceil(o.distance);
@@ -730,7 +767,8 @@ int find_peaks_impl(const float* x, int n, const bp_peak_options& o, const PeakO
                                                                         prom, lb, rb);
     BP_LAUNCHED("prominence_kernel");
     prominence_flags_kernel<<<grid_for((long long)m + 1, 256), 256, 0, st>>>(
-        prom, m, o.prominence_min, o.prominence_max, flags);
+        prom, pos, m, o.prominence_min, o.prominence_max, o.d_prominence_min,
+        o.d_prominence_max, flags);
     BP_LAUNCHED("prominence_flags_kernel");
     int* prank = nullptr;
     BP_TRY(sc.get(&prank, (size_t)m + 1));
@@ -755,6 +793,7 @@ bp_peak_options distance_only(double distance) {
   bp_peak_options o{};
   o.distance = distance;
   o.height_min = o.height_max = NAN;
+  o.threshold_min = o.threshold_max = NAN;
   o.prominence_min = o.prominence_max = NAN;
   return o;
 }

@@ -99,7 +99,7 @@ def _borders(interval, n, device):
         if v is None:
             return float("nan"), None
         if isinstance(v, np.ndarray) or _is_tensor(v):
-            a = _as_device(v, torch.float32).reshape(-1)
+            a = _as_device(v, torch.float64).reshape(-1)
             if a.numel() != n:
                 raise ValueError("array size of interval border must match x")
             return float("nan"), a
@@ -112,21 +112,26 @@ def _borders(interval, n, device):
 def find_peaks(x, height=None, threshold=None, distance=None, prominence=None, width=None,
                wlen=None, rel_height=0.5, plateau_size=None):
     """``(peaks, properties)`` as ``scipy.signal.find_peaks(x, height=,
-    distance=, prominence=, wlen=)``, with SciPy's parameter order;
-    ``threshold``, ``width`` and ``plateau_size`` are not implemented and
-    raise NotImplementedError when given.
+    threshold=, distance=, prominence=, wlen=)``, with SciPy's parameter
+    order; ``width`` and ``plateau_size`` are not implemented and raise
+    NotImplementedError when given.
 
     Peaks are the local maxima of x (a flat plateau counts at its midpoint
     when both its neighbours are lower), then, in SciPy's order: the height
-    condition (a number, a (min, max) pair, or per-sample arrays), the
-    minimum distance (peaks taken in decreasing height; every peak closer
+    condition, the threshold condition (the peak's rise over each neighbour:
+    the smaller rise against the lower border, the larger against the upper),
+    the minimum distance (peaks taken in decreasing height; every peak closer
     than ``ceil(distance)`` samples to a taken one is dropped; equal heights:
     the later sample first, where SciPy leaves the order to NumPy's unstable
-    sort), and the prominence condition (walks limited to ``wlen``).
-    properties: ``peak_heights`` with height; ``prominences``,
-    ``left_bases``, ``right_bases`` with prominence, as SciPy returns them.
+    sort), and the prominence condition (walks limited to ``wlen``).  Each
+    condition takes a number, a (min, max) pair with None for an open side,
+    or per-sample arrays read at the peaks, as SciPy does.
+    properties: ``peak_heights`` with height; ``left_thresholds``,
+    ``right_thresholds`` with threshold; ``prominences``, ``left_bases``,
+    ``right_bases`` with prominence, as SciPy returns them (float64 values,
+    int64 indexes).
     """
-    for name, v in (("threshold", threshold), ("width", width), ("plateau_size", plateau_size)):
+    for name, v in (("width", width), ("plateau_size", plateau_size)):
         if v is not None:
             raise NotImplementedError(f"find_peaks: `{name}` is not implemented on the GPU")
     lib = load_library("gpu")
@@ -142,23 +147,20 @@ def find_peaks(x, height=None, threshold=None, distance=None, prominence=None, w
     opt = PeakOptions()
     opt.distance = 0.0 if distance is None else float(distance)
     keep_alive = []
-    if height is not None:
-        opt.use_height = 1
-        opt.height_min, opt.height_max, lo_a, hi_a = _borders(height, n, d.device)
+    for name, cond in (("height", height), ("threshold", threshold),
+                       ("prominence", prominence)):
+        if cond is None:
+            setattr(opt, f"{name}_min", float("nan"))
+            setattr(opt, f"{name}_max", float("nan"))
+            continue
+        setattr(opt, f"use_{name}", 1)
+        lo, hi, lo_a, hi_a = _borders(cond, n, d.device)
         keep_alive += [lo_a, hi_a]
-        opt.d_height_min = None if lo_a is None else lo_a.data_ptr()
-        opt.d_height_max = None if hi_a is None else hi_a.data_ptr()
-    else:
-        opt.height_min = opt.height_max = float("nan")
-    if prominence is not None:
-        opt.use_prominence = 1
-        p_lo, p_hi, p_lo_a, p_hi_a = _borders(prominence, n, d.device)
-        if p_lo_a is not None or p_hi_a is not None:
-            raise NotImplementedError("find_peaks: array borders of `prominence`")
-        opt.prominence_min, opt.prominence_max = p_lo, p_hi
-        opt.wlen = 0.0 if wlen is None else float(wlen)
-    else:
-        opt.prominence_min = opt.prominence_max = float("nan")
+        setattr(opt, f"{name}_min", lo)
+        setattr(opt, f"{name}_max", hi)
+        setattr(opt, f"d_{name}_min", None if lo_a is None else lo_a.data_ptr())
+        setattr(opt, f"d_{name}_max", None if hi_a is None else hi_a.data_ptr())
+    opt.wlen = 0.0 if wlen is None else float(wlen)
     peaks = torch.empty(cap, dtype=torch.int32, device=d.device)
     prom = lb = rb = None
     if prominence is not None:
@@ -177,6 +179,11 @@ def find_peaks(x, height=None, threshold=None, distance=None, prominence=None, w
     props = {}
     if height is not None:
         props["peak_heights"] = d[p].to(torch.float64)
+    if threshold is not None:
+        # the rises of the kept peaks, exact float64 differences as SciPy's
+        xp = d[p].to(torch.float64)
+        props["left_thresholds"] = xp - d[p - 1].to(torch.float64)
+        props["right_thresholds"] = xp - d[p + 1].to(torch.float64)
     if prominence is not None:
         props["prominences"] = prom[:k]
         props["left_bases"] = lb[:k].to(torch.int64)

@@ -334,21 +334,28 @@ BP_API int bp_find_peaks_dev(const float *d_x, size_t n_samples, double distance
 
 /* SciPy's other find_peaks conditions used around the tutorial (the
  * prominence / wlen option is shown at notebooks/3_beampower.ipynb:625),
- * applied in SciPy's order: height, distance, prominence.  Borders are
- * float64 with NaN for an open side; d_height_min / d_height_max, when not
- * NULL, give per-sample borders read at the peak (SciPy's array borders). */
+ * applied in SciPy's order: height, threshold, distance, prominence.  Borders
+ * are float64 with NaN for an open side; the d_height_* / d_threshold_* /
+ * d_prominence_* arrays, when not NULL, give per-sample float64 borders (n_samples values)
+ * read at the peak (SciPy's array borders). */
 typedef struct bp_peak_options {
   double distance;          /* <= 0: no distance rule                          */
   int32_t use_height;       /* 1: keep height_min <= x[peak] <= height_max      */
   double height_min, height_max;
-  const float *d_height_min, *d_height_max;
+  const double *d_height_min, *d_height_max;
+  int32_t use_threshold;    /* 1: keep threshold_min <= min(x[p] - x[p-1],
+                               x[p] - x[p+1]) and max(...) <= threshold_max    */
+  double threshold_min, threshold_max;
+  const double *d_threshold_min, *d_threshold_max;
   int32_t use_prominence;   /* 1: keep prominence_min <= prominence <= max      */
   double prominence_min, prominence_max;
+  const double *d_prominence_min, *d_prominence_max;
   double wlen;              /* > 1: prominence walk limited to ceil(wlen) / 2
                                samples each side; <= 0: whole series            */
 } bp_peak_options;
 
-/* Peaks as scipy.signal.find_peaks(x, height=, distance=, prominence=, wlen=)
+/* Peaks as scipy.signal.find_peaks(x, height=, threshold=, distance=,
+ * prominence=, wlen=)
  * (identical indexes; prominences in float64, bases as SciPy's
  * left_bases / right_bases).  d_prominences / d_left_bases / d_right_bases
  * may be NULL and are written only with use_prominence.  Synchronises. */

@@ -22,11 +22,12 @@ SciPy (1.18.1 in this image) is a third-party dependency of the tutorial.  Its
 peak finder is restated here from its published algorithm
 (scipy/signal/_peak_finding_utils.pyx: ``_local_maxima_1d``,
 ``_select_by_peak_distance``, ``_peak_prominences``; scipy/signal/
-_peak_finding.py: the height / prominence conditions), and the tests compare
-this restatement with SciPy itself.  The tutorial uses ``distance`` and shows
-``prominence`` with ``wlen`` as an option (notebooks/3_beampower.ipynb:625).  Where SciPy orders equal peak heights through NumPy's
-(unstable) default argsort, this restatement uses the stable order: among
-equal heights the later sample is considered first.
+_peak_finding.py: the height / threshold / prominence conditions), and the
+tests compare this restatement with SciPy itself.  The tutorial uses
+``distance`` and shows ``prominence`` with ``wlen`` as an option
+(notebooks/3_beampower.ipynb:625).  Where SciPy orders equal peak heights
+through NumPy's (unstable) default argsort, this restatement uses the stable
+order: among equal heights the later sample is considered first.
 """
 from __future__ import annotations
 
@@ -196,11 +197,13 @@ def peak_prominences(x, peaks, wlen=None):
     return prom, lb, rb
 
 
-def find_peaks(x, distance=None, height=None, prominence=None, wlen=None, properties=False):
-    """Peaks of x as scipy.signal.find_peaks(x, height=, distance=,
-    prominence=, wlen=): local maxima, then the height condition, the
-    distance rule and the prominence condition, in SciPy's order.  Returns
-    the indexes, or (indexes, properties) with ``properties=True``."""
+def find_peaks(x, distance=None, height=None, prominence=None, wlen=None, properties=False,
+               threshold=None):
+    """Peaks of x as scipy.signal.find_peaks(x, height=, threshold=,
+    distance=, prominence=, wlen=): local maxima, then the height condition,
+    the threshold condition, the distance rule and the prominence condition,
+    in SciPy's order.  Returns the indexes, or (indexes, properties) with
+    ``properties=True``."""
     x = np.asarray(x)
     if x.ndim != 1:
         raise ValueError("x must be one-dimensional")
@@ -213,6 +216,20 @@ def find_peaks(x, distance=None, height=None, prominence=None, wlen=None, proper
         keep = within(h, lo, hi)
         peaks = peaks[keep]
         props["peak_heights"] = h[keep]
+    if threshold is not None:
+        # the rise over each neighbour; the smaller one against the lower
+        # border, the larger one against the upper border
+        left = x64[peaks] - x64[peaks - 1]
+        right = x64[peaks] - x64[peaks + 1]
+        lo, hi = interval_borders(threshold, x64, peaks)
+        keep = np.ones(peaks.size, dtype=bool)
+        if lo is not None:
+            keep &= lo <= np.minimum(left, right)
+        if hi is not None:
+            keep &= np.maximum(left, right) <= hi
+        peaks = peaks[keep]
+        props = {k: v[keep] for k, v in props.items()}
+        props.update(left_thresholds=left[keep], right_thresholds=right[keep])
     if distance is not None:
         if distance < 1:
             raise ValueError("distance must be greater or equal to 1")

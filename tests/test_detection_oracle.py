@@ -91,14 +91,24 @@ def test_pairwise_sum_tree_matches_numpy(bplib):
     {"height": 0.2}, {"height": (0.1, 0.6)}, {"height": "array"},
     {"prominence": 0.3}, {"prominence": (0.2, 1.5), "wlen": 25},
     {"prominence": 0.1, "wlen": 7.5}, {"height": 0.0, "distance": 40, "prominence": 0.25},
-    {"distance": 12, "prominence": (None, 0.8), "wlen": 100}])
+    {"distance": 12, "prominence": (None, 0.8), "wlen": 100},
+    {"threshold": 0.02}, {"threshold": (0.01, 0.2)}, {"threshold": (None, 0.05)},
+    {"threshold": "array", "distance": 8}, {"height": 0.1, "threshold": 0.01, "prominence": 0.2},
+    {"prominence": "array", "wlen": 60}, {"prominence": ("array", 2.0)}])
 def test_oracle_peak_options_match_scipy(seed, kw):
     rng = np.random.default_rng(seed)
     x = np.convolve(rng.standard_normal(4000), np.ones(5) / 5, mode="same").astype(np.float32)
     x[700:706] = x[700]
     kw = dict(kw)
+    wave = 0.1 + 0.2 * np.sin(np.arange(x.size) / 300.0)
     if kw.get("height") == "array":
-        kw["height"] = (0.1 + 0.2 * np.sin(np.arange(x.size) / 300.0)).astype(np.float32)
+        kw["height"] = wave.astype(np.float32)
+    if kw.get("threshold") == "array":
+        kw["threshold"] = 0.1 * wave  # float64 borders, compared in float64
+    if kw.get("prominence") == "array":
+        kw["prominence"] = 2.0 * wave
+    if isinstance(kw.get("prominence"), tuple) and kw["prominence"][0] == "array":
+        kw["prominence"] = (wave, kw["prominence"][1])
     ref, ref_props = signal.find_peaks(x, **kw)
     got, props = odet.find_peaks(x, properties=True, **kw)
     assert np.array_equal(got, ref)

@@ -136,7 +136,10 @@ def test_edge_cases(cuda):
     {"height": 0.2}, {"height": (0.1, 0.6)}, {"height": "array"},
     {"prominence": 0.3}, {"prominence": (0.2, 1.5), "wlen": 25},
     {"prominence": 0.1, "wlen": 7.5}, {"height": 0.0, "distance": 40, "prominence": 0.25},
-    {"distance": 12, "prominence": (None, 0.8), "wlen": 100}])
+    {"distance": 12, "prominence": (None, 0.8), "wlen": 100},
+    {"threshold": 0.02}, {"threshold": (0.01, 0.2)}, {"threshold": (None, 0.05)},
+    {"threshold": "array", "distance": 8}, {"height": 0.1, "threshold": 0.01, "prominence": 0.2},
+    {"prominence": "array", "wlen": 60}, {"prominence": ("array", 2.0)}])
 def test_peak_options_match_oracle(cuda, seed, kw):
     """height / prominence / wlen (the tutorial's commented option at
     notebooks/3_beampower.ipynb:625): identical peaks and properties."""
@@ -146,8 +149,15 @@ def test_peak_options_match_oracle(cuda, seed, kw):
     x[700:706] = x[700]
     x[9000:9400] = 0.0
     kw = dict(kw)
+    wave = 0.1 + 0.2 * np.sin(np.arange(x.size) / 300.0)
     if kw.get("height") == "array":
-        kw["height"] = (0.1 + 0.2 * np.sin(np.arange(x.size) / 300.0)).astype(np.float32)
+        kw["height"] = wave.astype(np.float32)
+    if kw.get("threshold") == "array":
+        kw["threshold"] = 0.1 * wave  # float64 borders, compared in float64
+    if kw.get("prominence") == "array":
+        kw["prominence"] = 2.0 * wave
+    if isinstance(kw.get("prominence"), tuple) and kw["prominence"][0] == "array":
+        kw["prominence"] = (wave, kw["prominence"][1])
     ref, ref_props = odet.find_peaks(x, properties=True, **kw)
     got, props = _det().find_peaks(x, **kw)
     assert np.array_equal(got, ref)
