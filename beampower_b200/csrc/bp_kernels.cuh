@@ -459,6 +459,12 @@ struct Staged {
         }
         sm.meta_s[i] = m;
       }
+      // Per source slot: {source, first, end, 0} with [first, end) the
+      // record-local samples the out-of-bounds rule keeps (strict: every
+      // delay of the source inside the record, the lower bound in global
+      // time); empty for an unused slot.  Bounds are clamped to +-2^30,
+      // beyond any sample index of a record.
+      constexpr long long kFar = 1ll << 30;
       for (int i = tid; i < K; i += blockDim.x) {
         int4 si = tb.src_info[(size_t)tile * K + i];
         if (rc.srcmm) {
@@ -466,7 +472,15 @@ struct Staged {
           si.y = mm.x;
           si.z = mm.y;
         }
-        sm.srci[i] = si;
+        long long first = -kFar, end = kFar;
+        if (si.x < 0 || (!rc.flexible && si.y > si.z)) {
+          first = kFar;
+          end = -kFar;
+        } else if (!rc.flexible) {
+          first = min(max(-rc.t_origin - (long long)si.y, -kFar), kFar);
+          end = min(max((long long)rc.T - (long long)si.z, -kFar), kFar);
+        }
+        sm.srci[i] = make_int4(si.x, (int)first, (int)end, 0);
       }
     }
     __syncthreads();  // the meta copy above read st_s[] as table slots
@@ -709,28 +723,30 @@ struct Staged {
 
       // ---- epilogue of the time tile ----
       if constexpr (MAXRED) {
+        // source-major: each slot read once; the best key per sample stays in
+        // registers while the accumulators of processed sources die
+        unsigned long long best[MT / 2][2];
 #pragma unroll
-        for (int q = 0; q < MT / 2; ++q) {
+        for (int q = 0; q < MT / 2; ++q) best[q][0] = best[q][1] = 0ull;
 #pragma unroll
-          for (int h = 0; h < 2; ++h) {
-            const int rel = pair_sample<STORAGE>(lane, q, h);
-            const long long t = (long long)t0 + rel;
-            const long long g = rc.t_origin + t;
-            unsigned long long best = 0ull;
+        for (int k = 0; k < KS; ++k) {
+          const int4 si = my_src[k];
 #pragma unroll
-            for (int k = 0; k < KS; ++k) {
-              const int4 si = my_src[k];
-              if (si.x < 0) continue;
-              const bool valid =
-                  rc.flexible ? true
-                              : (si.y <= si.z && g + si.y >= 0 && t + (long long)si.z < rc.T);
-              if (!valid) continue;
+          for (int q = 0; q < MT / 2; ++q) {
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+              const int t = t0 + pair_sample<STORAGE>(lane, q, h);
+              if (t < si.y || t >= si.z) continue;  // outside the kept samples (or no source)
               const unsigned long long key = make_key(h ? acc[k][q].y : acc[k][q].x, si.x);
-              best = key > best ? key : best;
+              best[q][h] = key > best[q][h] ? key : best[q][h];
             }
-            sm.red[warp * TT + rel] = best;
           }
         }
+#pragma unroll
+        for (int q = 0; q < MT / 2; ++q)
+#pragma unroll
+          for (int h = 0; h < 2; ++h)
+            sm.red[warp * TT + pair_sample<STORAGE>(lane, q, h)] = best[q][h];
         named_barrier_sync(1, NCONS);
         for (int i = tid; i < TT; i += NCONS) {
           unsigned long long best = 0ull;
@@ -753,13 +769,9 @@ struct Staged {
           for (int q = 0; q < MT / 2; ++q) {
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
-              const long long t = (long long)t0 + pair_sample<STORAGE>(lane, q, h);
+              const int t = t0 + pair_sample<STORAGE>(lane, q, h);
               if (t < rc.out0 || t >= rc.out1) continue;
-              const long long g = rc.t_origin + t;
-              const bool valid =
-                  rc.flexible ? true
-                              : (si.y <= si.z && g + si.y >= 0 && t + (long long)si.z < rc.T);
-              if (valid) row[t] = h ? acc[k][q].y : acc[k][q].x;
+              if (t >= si.y && t < si.z) row[t] = h ? acc[k][q].y : acc[k][q].x;
             }
           }
         }
