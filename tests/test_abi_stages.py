@@ -45,6 +45,34 @@ def test_peaks_and_detect_reject(lib):
                              None) == INVALID
 
 
+def test_peak_options_reject(lib):
+    """bp_find_peaks_opt_dev: SciPy's argument errors, before any CUDA work."""
+    from beampower_b200.core import PeakOptions
+    buf = ct.c_void_p(1)
+    n = ct.c_size_t(123)
+
+    def opts(**kw):
+        o = PeakOptions()
+        for name in ("height", "threshold", "prominence"):
+            setattr(o, f"{name}_min", float("nan"))
+            setattr(o, f"{name}_max", float("nan"))
+        for k, v in kw.items():
+            setattr(o, k, v)
+        return o
+
+    def call(o, cap=50, count=ct.byref(n)):
+        return lib.bp_find_peaks_opt_dev(buf, 100, None if o is None else ct.byref(o), buf,
+                                         None, None, None, cap, count, None)
+
+    assert call(None) == INVALID                                   # no options
+    assert call(opts(), count=None) == INVALID                     # no count
+    assert call(opts(distance=0.5)) == INVALID and n.value == 0    # 0 < distance < 1
+    assert call(opts(use_prominence=1, wlen=1.0)) == INVALID       # ceil(wlen) <= 1
+    assert call(opts(), cap=49) == INVALID                         # capacity < n / 2
+    assert lib.bp_find_peaks_opt_dev(None, 100, ct.byref(opts()), buf, None, None, None, 50,
+                                     ct.byref(n), None) == INVALID  # NULL series
+
+
 def test_features_and_ingest_reject_or_empty(lib):
     buf = ct.c_void_p(1)
     assert lib.bp_envelope_dev(None, 2, 10, 1e5, buf, None) == INVALID
