@@ -32,14 +32,31 @@ _i32p = ct.POINTER(ct.c_int)
 _sz = ct.c_size_t
 
 
-def build(reference_root: str | None = "/root/reference") -> None:
-    """Compile the oracle (and the reference libraries when the reference
-    sources are present)."""
+REFERENCE_ENV = "BEAMPOWER_REFERENCE"
+
+
+def reference_checkout() -> str | None:
+    """The reference checkout, when one is present: the directory named by the
+    BEAMPOWER_REFERENCE environment variable, else a checkout named
+    ``reference`` beside this repository; None when neither holds the
+    reference's sources."""
+    repo = os.path.dirname(HERE)
+    for cand in (os.environ.get(REFERENCE_ENV),
+                 os.path.join(os.path.dirname(repo), "reference")):
+        if cand and os.path.isdir(os.path.join(cand, "beampower", "src")):
+            return cand
+    return None
+
+
+def build(reference_root: str | None = None) -> None:
+    """Compile the oracle, and the reference libraries when `reference_root`
+    (a reference checkout) holds the reference's sources."""
     targets = ["oracle"]
+    args = []
     if reference_root and os.path.isdir(os.path.join(reference_root, "beampower", "src")):
         targets.append("ref")
-    subprocess.run(["make", "-s", "-C", HERE, f"REF_ROOT={reference_root}"] + targets,
-                   check=True)
+        args.append(f"REF_ROOT={reference_root}")
+    subprocess.run(["make", "-s", "-C", HERE, *args] + targets, check=True)
 
 
 def _fp(a):

@@ -71,7 +71,10 @@ def cases(rng):
 
 
 def main():
-    ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref_root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("BEAMPOWER_REFERENCE")
+    if not ref_root:
+        sys.exit(f"usage: python {os.path.basename(__file__)} <reference checkout> "
+                 "(or set BEAMPOWER_REFERENCE)")
     tdt = load_threshold_function(ref_root)
     rng = np.random.default_rng(2024)
     for i, (name, (x, W, ov, kind, nd, dist)) in enumerate(cases(rng).items()):

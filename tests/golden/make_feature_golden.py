@@ -60,7 +60,10 @@ def traces(rng):
 
 
 def main():
-    ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref_root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("BEAMPOWER_REFERENCE")
+    if not ref_root:
+        sys.exit(f"usage: python {os.path.basename(__file__)} <reference checkout> "
+                 "(or set BEAMPOWER_REFERENCE)")
     envelope = load_envelope(ref_root)
     res = {}
     for name, x in traces(np.random.default_rng(77)).items():

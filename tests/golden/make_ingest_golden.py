@@ -31,7 +31,10 @@ def load_sec_to_samp(ref_root):
 
 
 def main():
-    ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref_root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("BEAMPOWER_REFERENCE")
+    if not ref_root:
+        sys.exit(f"usage: python {os.path.basename(__file__)} <reference checkout> "
+                 "(or set BEAMPOWER_REFERENCE)")
     f = load_sec_to_samp(ref_root)
     rng = np.random.default_rng(99)
     tt = rng.uniform(0.0, 60.0, size=(300, 12, 2)).astype(np.float32)
