@@ -1,8 +1,9 @@
 """Autotuner of the staged kernel's shape.
 
 The library compiles the staged kernel in several shapes (sources per
-thread, samples per lane, consumer warps, ring stages; see
-``bp_kernel_config_describe``), all over the same 64-source tables.  Which is
+thread, samples per lane, consumer warps, ring stages, stations per ring
+stage, sources per block; see ``bp_kernel_config_describe`` and
+``bp_kernel_config_shape``), all over the same 64-source tables.  Which is
 fastest depends on the storage type (FP32 is shared-memory bound, 16-bit
 storage issue bound), the number of phases and the tables' delay spread.
 ``autotune`` times every shape on the caller's own table and traces, keeps
@@ -27,14 +28,18 @@ def cache_path():
 
 
 def configs():
-    """[(id, {sources_per_thread, samples_per_lane, consumer_warps, stages})]."""
+    """[(id, {sources_per_thread, samples_per_lane, consumer_warps, stages,
+    stations_per_stage, sources_per_block, blocks_per_sm})]."""
     lib = load_library("gpu")
     out = []
     for c in range(lib.bp_kernel_config_count()):
         v = [ct.c_int() for _ in range(4)]
         check(lib.bp_kernel_config_describe(c, *[ct.byref(x) for x in v]))
+        x = [ct.c_int() for _ in range(3)]
+        check(lib.bp_kernel_config_shape(c, *[ct.byref(y) for y in x]))
         out.append((c, dict(zip(("sources_per_thread", "samples_per_lane", "consumer_warps",
-                                 "stages"), (x.value for x in v)))))
+                                 "stages", "stations_per_stage", "sources_per_block",
+                                 "blocks_per_sm"), [y.value for y in v + x]))))
     return out
 
 

@@ -142,6 +142,8 @@ SIGNATURES = {
     "bp_kernel_config_count": ([], _int),
     "bp_kernel_config_describe": ([_int, ct.POINTER(_int), ct.POINTER(_int), ct.POINTER(_int),
                                    ct.POINTER(_int)], _int),
+    "bp_kernel_config_shape": ([_int, ct.POINTER(_int), ct.POINTER(_int), ct.POINTER(_int)],
+                               _int),
     "bp_set_kernel_config": ([_int, _int, _int], _int),
     "bp_get_kernel_config": ([_int, _int], _int),
     "bp_debug_wait_timeout": ([ct.c_ulonglong, _vp, ct.POINTER(_int)], _int),

@@ -81,17 +81,22 @@ namespace {
 inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 
 struct CfgDesc {
-  int ks, mt, ws, nstage;
+  int ks, mt, ws, nstage, sps, k, minb;
 };
 template <int ID>
 constexpr CfgDesc cfg_desc() {
-  return {KCfg<ID>::KS, KCfg<ID>::MT, KCfg<ID>::WS, KCfg<ID>::NSTAGE};
+  using C = KCfg<ID>;
+  return {C::KS, C::MT, C::WS, C::NSTAGE, C::SPS, C::K, C::MINB};
 }
-constexpr CfgDesc kCfgDesc[kNumConfigs] = {cfg_desc<0>(), cfg_desc<1>()};
+constexpr CfgDesc kCfgDesc[kNumConfigs] = {cfg_desc<0>(), cfg_desc<1>(), cfg_desc<2>(),
+                                           cfg_desc<3>(), cfg_desc<4>(), cfg_desc<5>()};
 
-inline int cfg_time_tile(int cfg) {
-  return 32 * kCfgDesc[(cfg >= 0 && cfg < kNumConfigs) ? cfg : 0].mt;
+inline const CfgDesc& cfg_of(int cfg) {
+  return kCfgDesc[(cfg >= 0 && cfg < kNumConfigs) ? cfg : 0];
 }
+inline int cfg_time_tile(int cfg) { return 32 * cfg_of(cfg).mt; }
+// Blocks that share one 64-source table tile.
+inline int cfg_blocks_per_tile(int cfg) { return kTileSources / cfg_of(cfg).k; }
 
 // Preferred config per (storage, reduce); -1 = built-in default.
 std::atomic<int> g_cfg_choice[3][2] = {{{-1}, {-1}}, {{-1}, {-1}}, {{-1}, {-1}}};
@@ -268,9 +273,14 @@ int build_tiling_map(const int32_t* d_delays, const float* d_w, size_t N, size_t
 template <bool MAXRED>
 int launch_window(int cfg, int P, bool checked, int storage, const bp::LaunchArgs& a,
                   bool batch, long long blocks, int dev, cudaStream_t st) {
-  if (cfg == 1)
-    return launch_window_c<1, MAXRED>(P, checked, storage, a, batch, blocks, dev, st);
-  return launch_window_c<0, MAXRED>(P, checked, storage, a, batch, blocks, dev, st);
+  switch (cfg) {
+    case 1: return launch_window_c<1, MAXRED>(P, checked, storage, a, batch, blocks, dev, st);
+    case 2: return launch_window_c<2, MAXRED>(P, checked, storage, a, batch, blocks, dev, st);
+    case 3: return launch_window_c<3, MAXRED>(P, checked, storage, a, batch, blocks, dev, st);
+    case 4: return launch_window_c<4, MAXRED>(P, checked, storage, a, batch, blocks, dev, st);
+    case 5: return launch_window_c<5, MAXRED>(P, checked, storage, a, batch, blocks, dev, st);
+    default: return launch_window_c<0, MAXRED>(P, checked, storage, a, batch, blocks, dev, st);
+  }
 }
 
 template <int CFG>
@@ -279,11 +289,11 @@ size_t staged_smem_cfg(int P, bool maxred, int rowcap, int max_active, int row_f
   auto f = [&](auto tag) -> size_t {
     constexpr int PP = decltype(tag)::value;
     if (maxred)
-      return bp::WindowSmem<PP, C::KS, C::MT, C::WS, C::NSTAGE, true>(rowcap, max_active,
-                                                                       row_factor)
+      return bp::WindowSmem<PP, C::KS, C::MT, C::WS, C::NSTAGE, C::SPS, true>(
+                 rowcap, max_active, row_factor)
           .total;
-    return bp::WindowSmem<PP, C::KS, C::MT, C::WS, C::NSTAGE, false>(rowcap, max_active,
-                                                                      row_factor)
+    return bp::WindowSmem<PP, C::KS, C::MT, C::WS, C::NSTAGE, C::SPS, false>(
+               rowcap, max_active, row_factor)
         .total;
   };
   switch (P) {
@@ -299,8 +309,14 @@ size_t staged_smem_cfg(int P, bool maxred, int rowcap, int max_active, int row_f
 size_t staged_smem_bytes(int cfg, int P, bool maxred, int rowcap, int max_active, int storage) {
   const int rf = storage == BP_STORAGE_F32 ? bp::ring_row_factor<BP_STORAGE_F32>()
                                            : bp::ring_row_factor<BP_STORAGE_F16>();
-  if (cfg == 1) return staged_smem_cfg<1>(P, maxred, rowcap, max_active, rf);
-  return staged_smem_cfg<0>(P, maxred, rowcap, max_active, rf);
+  switch (cfg) {
+    case 1: return staged_smem_cfg<1>(P, maxred, rowcap, max_active, rf);
+    case 2: return staged_smem_cfg<2>(P, maxred, rowcap, max_active, rf);
+    case 3: return staged_smem_cfg<3>(P, maxred, rowcap, max_active, rf);
+    case 4: return staged_smem_cfg<4>(P, maxred, rowcap, max_active, rf);
+    case 5: return staged_smem_cfg<5>(P, maxred, rowcap, max_active, rf);
+    default: return staged_smem_cfg<0>(P, maxred, rowcap, max_active, rf);
+  }
 }
 
 int rowcap_for(const bp_table* t, int cfg) {
@@ -375,13 +391,14 @@ int run_staged(const bp_table* t, const void* traces, int storage, const float* 
   const int cfg = config_for(t, storage, maxred);
   const int tt = cfg_time_tile(cfg);
   const int n_tt = (int)((T + tt - 1) / tt);
-  a.tiles_per_chunk = choose_tiles_per_chunk(n_tt, t->dev.n_tiles, t->device);
+  const int n_btiles = t->dev.n_tiles * cfg_blocks_per_tile(cfg);
+  a.tiles_per_chunk = choose_tiles_per_chunk(n_tt, n_btiles, t->device);
   a.rowcap = rowcap_for(t, cfg);
   a.max_active = std::max(1, t->info.max_active);
   a.status = t->status;
   if (n_tt == 0) return BP_OK;
   const long long blocks =
-      (long long)((n_tt + a.tiles_per_chunk - 1) / a.tiles_per_chunk) * t->dev.n_tiles;
+      (long long)((n_tt + a.tiles_per_chunk - 1) / a.tiles_per_chunk) * n_btiles;
   const bool checked = out_of_bounds && t->info.any_nonfinite;
   if (maxred)
     return launch_window<true>(cfg, t->dev.P, checked, storage, a, false, blocks, t->device, st);
@@ -1185,7 +1202,8 @@ int bp_batch_create(const bp_table* const* tables, int n_tables, const bp_record
     v.station_mask = q.station_mask;
     v.beam_max = q.beam_max;
     v.argmax = q.argmax;
-    prefix[r + 1] = prefix[r] + (long long)v.n_chunks * t->dev.n_tiles;
+    prefix[r + 1] =
+        prefix[r] + (long long)v.n_chunks * t->dev.n_tiles * cfg_blocks_per_tile(cfg);
     n_keys += q.out1 - q.out0;
     if (q.station_mask) n_srcmm += (size_t)t->dev.n_tiles * kTileSources;
   }
@@ -1339,12 +1357,13 @@ int bp_record_beamform_max_dev(const bp_table* t, const bp_record* q, int storag
   const int tt = cfg_time_tile(cfg);
   const int tau_first = r.out0 / tt;
   const int n_tt = (r.out1 + tt - 1) / tt - tau_first;
-  a.tiles_per_chunk = choose_tiles_per_chunk(n_tt, t->dev.n_tiles, t->device);
+  const int n_btiles = t->dev.n_tiles * cfg_blocks_per_tile(cfg);
+  a.tiles_per_chunk = choose_tiles_per_chunk(n_tt, n_btiles, t->device);
   a.rowcap = rowcap_for(t, cfg);
   a.max_active = std::max(1, t->info.max_active);
   a.status = t->status;
   const long long blocks =
-      (long long)((n_tt + a.tiles_per_chunk - 1) / a.tiles_per_chunk) * t->dev.n_tiles;
+      (long long)((n_tt + a.tiles_per_chunk - 1) / a.tiles_per_chunk) * n_btiles;
   const bool checked = q->out_of_bounds && t->info.any_nonfinite;
   if (int rc = launch_window<true>(cfg, t->dev.P, checked, storage, a, false, blocks, t->device,
                                    st))
@@ -1376,6 +1395,16 @@ int bp_kernel_config_describe(int cfg, int* sources_per_thread, int* samples_per
   if (samples_per_lane) *samples_per_lane = d.mt;
   if (consumer_warps) *consumer_warps = d.ws;
   if (stages) *stages = d.nstage;
+  return BP_OK;
+}
+
+int bp_kernel_config_shape(int cfg, int* stations_per_stage, int* sources_per_block,
+                           int* blocks_per_sm) {
+  if (cfg < 0 || cfg >= kNumConfigs) return fail(BP_ERR_INVALID_ARGUMENT, "no config %d", cfg);
+  const CfgDesc& d = kCfgDesc[cfg];
+  if (stations_per_stage) *stations_per_stage = d.sps;
+  if (sources_per_block) *sources_per_block = d.k;
+  if (blocks_per_sm) *blocks_per_sm = d.minb;
   return BP_OK;
 }
 

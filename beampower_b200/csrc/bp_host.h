@@ -43,27 +43,33 @@ void retain_pool(int dev);
 constexpr long long kMaxInt = std::numeric_limits<int>::max();
 
 // ---- staged-kernel configurations --------------------------------------------
-// All use 64-source tiles (the table's tile size).  Config 0: 8 consumer warps
-// x 8 sources per thread, 8 samples per lane (256-sample time tiles), 2 blocks
-// per SM.  Config 1: 16 consumer warps x 4 sources, 16 samples per lane
-// (512-sample time tiles), 1 block per SM: twice the terms per metadata load.
-// (A third shape, 16 warps x 4 sources x 8 samples at 2 blocks per SM, was
+// Each covers the table's 64-source tiles with WS consumer warps x KS sources
+// per thread (one block per tile, or two blocks of 32 sources when WS x KS is
+// 32), MT samples per lane (time tiles of 32 MT samples), SPS stations per
+// ring stage, and MINB blocks per SM.
+//   0: 8 x 8, MT 8,  SPS 1, 2/SM     1: 16 x 4, MT 16, SPS 1, 1/SM
+//   2: 16 x 4, MT 16, SPS 2, 1/SM    3: 8 x 8, MT 8,  SPS 2, 2/SM
+//   4: 16 x 2, MT 32, SPS 1, 1/SM    5: 16 x 2, MT 32, SPS 2, 1/SM
+// (A shape of 16 warps x 4 sources x 8 samples at 2 blocks per SM was
 // measured slower for every storage type: capped at 56 registers it spills.)
 #ifndef BP_NSTAGE
 #define BP_NSTAGE 4
 #endif
+template <int WS_, int KS_, int MT_, int SPS_, int MINB_>
+struct KShape {
+  static constexpr int WS = WS_, KS = KS_, MT = MT_, SPS = SPS_, MINB = MINB_;
+  static constexpr int NSTAGE = BP_NSTAGE;
+  static constexpr int K = WS * KS;  // sources per block
+};
 template <int ID> struct KCfg;
-template <> struct KCfg<0> {
-  static constexpr int KS = 8, MT = 8, WS = 8, NSTAGE = BP_NSTAGE, MINB = 2;
-};
-template <> struct KCfg<1> {
-  static constexpr int KS = 4, MT = 16, WS = 16, NSTAGE = BP_NSTAGE, MINB = 1;
-};
-constexpr int kNumConfigs = 2;
-constexpr int kTileSources = 64;
-static_assert(KCfg<0>::KS * KCfg<0>::WS == kTileSources, "tile size");
-static_assert(KCfg<1>::KS * KCfg<1>::WS == kTileSources, "tile size");
-
+template <> struct KCfg<0> : KShape<8, 8, 8, 1, 2> {};
+template <> struct KCfg<1> : KShape<16, 4, 16, 1, 1> {};
+template <> struct KCfg<2> : KShape<16, 4, 16, 2, 1> {};
+template <> struct KCfg<3> : KShape<8, 8, 8, 2, 2> {};
+template <> struct KCfg<4> : KShape<16, 2, 32, 1, 1> {};
+template <> struct KCfg<5> : KShape<16, 2, 32, 2, 1> {};
+constexpr int kNumConfigs = 6;
+constexpr int kTileSources = bp::kTableTile;
 
 // Launches the staged kernel of config CFG (plain grid of `blocks` blocks, or
 // the persistent batch kernel when `batch`), choosing the template variant by
@@ -72,14 +78,18 @@ template <int CFG, bool MAXRED>
 int launch_window_c(int P, bool checked, int storage, const bp::LaunchArgs& a, bool batch,
                     long long blocks, int dev, cudaStream_t st);
 
-extern template int launch_window_c<0, true>(int, bool, int, const bp::LaunchArgs&, bool,
-                                             long long, int, cudaStream_t);
-extern template int launch_window_c<0, false>(int, bool, int, const bp::LaunchArgs&, bool,
-                                              long long, int, cudaStream_t);
-extern template int launch_window_c<1, true>(int, bool, int, const bp::LaunchArgs&, bool,
-                                             long long, int, cudaStream_t);
-extern template int launch_window_c<1, false>(int, bool, int, const bp::LaunchArgs&, bool,
-                                              long long, int, cudaStream_t);
+#define BP_EXTERN_CFG(C)                                                                  \
+  extern template int launch_window_c<C, true>(int, bool, int, const bp::LaunchArgs&, bool, \
+                                               long long, int, cudaStream_t);             \
+  extern template int launch_window_c<C, false>(int, bool, int, const bp::LaunchArgs&,      \
+                                                bool, long long, int, cudaStream_t);
+BP_EXTERN_CFG(0)
+BP_EXTERN_CFG(1)
+BP_EXTERN_CFG(2)
+BP_EXTERN_CFG(3)
+BP_EXTERN_CFG(4)
+BP_EXTERN_CFG(5)
+#undef BP_EXTERN_CFG
 
 }  // namespace bp_host
 

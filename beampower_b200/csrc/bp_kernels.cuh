@@ -294,6 +294,11 @@ struct LaunchArgs {
   int* status;
 };
 
+// Sources of a table tile (the tiling map groups sources by this many).  A
+// kernel configuration covers a tile with one block (WS * KS == kTableTile)
+// or splits it over kTableTile / (WS * KS) blocks.
+constexpr int kTableTile = 64;
+
 template <int P, int KS, int MT, int WS>
 struct WindowCfg {
   static constexpr int K = WS * KS;
@@ -305,18 +310,18 @@ __host__ __device__ inline size_t align_up_sz(size_t v, size_t a) { return (v + 
 
 // Shared-memory carve-up, used identically by host (size) and device.  A
 // ring row holds `rowcap` FP32 elements, or `rowcap` 16-bit elements of
-// each of the two versions: 4 * rowcap bytes either way.
-template <int P, int KS, int MT, int WS, int NSTAGE, bool MAXRED>
+// each of the kHalfCopies copies; a stage holds SPS stations x P rows.
+template <int P, int KS, int MT, int WS, int NSTAGE, int SPS, bool MAXRED>
 struct WindowSmem {
   using M = typename MetaT<P>::type;
   static constexpr int K = WS * KS;
   static constexpr int TT = 32 * MT;
-  size_t ring, meta, red, srci, st_s, st_lo, st_w, st_sc, bars, misc, total;
+  size_t ring, meta, red, srci, st_s, st_j, st_lo, st_w, st_sc, bars, misc, total;
   // row_factor: 32-bit words per ring row per sample of capacity
   // (ring_row_factor<STORAGE>())
   __host__ __device__ WindowSmem(int rowcap, int max_active, int row_factor) {
     size_t o = 0;
-    ring = o;        o += (size_t)NSTAGE * P * rowcap * 4 * row_factor;
+    ring = o;        o += (size_t)NSTAGE * SPS * P * rowcap * 4 * row_factor;
     o = align_up_sz(o, 16);
     meta = o;        o += (size_t)max_active * K * sizeof(M);
     o = align_up_sz(o, 16);
@@ -324,6 +329,7 @@ struct WindowSmem {
     o = align_up_sz(o, 16);
     srci = o;        o += (size_t)K * sizeof(int4);
     st_s = o;        o += (size_t)max_active * sizeof(int);
+    st_j = o;        o += (size_t)max_active * sizeof(int);
     st_lo = o;       o += (size_t)max_active * P * sizeof(int);
     st_w = o;        o += (size_t)max_active * P * sizeof(int);
     st_sc = o;       o += (size_t)max_active * sizeof(float);
@@ -343,21 +349,90 @@ __device__ __forceinline__ int pair_sample(int lane, int q, int h) {
   else return 4 * lane + 128 * (q >> 1) + 2 * (q & 1) + h;
 }
 
-// The staged shift-and-stack for one item (record, source tile, time tiles
-// [tau0, tau1)), shared by the plain and the persistent kernels.
-template <int P, int KS, int MT, int WS, int NSTAGE, bool MAXRED, bool CHECKED, int STORAGE>
+// ---- 16-bit arithmetic with FP32 accumulation --------------------------------
+// Packed FP16 pair add, round to nearest (no multiply precedes it).
+__device__ __forceinline__ uint32_t hadd2_rn(uint32_t a, uint32_t b) {
+  uint32_t d;
+  asm("add.rn.f16x2 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b));
+  return d;
+}
+
+// acc.{x,y} = round_f32(v.{lo,hi} * c.lo + acc.{x,y}) for FP16 v and c: the
+// mixed-precision FMA (16-bit sources, FP32 addend and result, one
+// rounding), which needs no widening of v.  The product of two FP16 values
+// is exact in FP32, so each lane equals fmaf((float)v, (float)c, acc).
+__device__ __forceinline__ void fma2_f32_f16(float2& acc, uint32_t v, uint32_t c) {
+  asm("{\n\t.reg .b16 vl, vh, cl, ch;\n\t"
+      "mov.b32 {vl, vh}, %2;\n\t"
+      "mov.b32 {cl, ch}, %3;\n\t"
+      "fma.rn.f32.f16 %0, vl, cl, %0;\n\t"
+      "fma.rn.f32.f16 %1, vh, cl, %1;\n\t}"
+      : "+f"(acc.x), "+f"(acc.y)
+      : "r"(v), "r"(c));
+}
+
+// The same for BF16 v and c (the product of two BF16 values is exact too).
+__device__ __forceinline__ void fma2_f32_bf16(float2& acc, uint32_t v, uint32_t c) {
+  asm("{\n\t.reg .b16 vl, vh, cl, ch;\n\t"
+      "mov.b32 {vl, vh}, %2;\n\t"
+      "mov.b32 {cl, ch}, %3;\n\t"
+      "fma.rn.f32.bf16 %0, vl, cl, %0;\n\t"
+      "fma.rn.f32.bf16 %1, vh, cl, %1;\n\t}"
+      : "+f"(acc.x), "+f"(acc.y)
+      : "r"(v), "r"(c));
+}
+
+// The factor c = w * scale of one (source, station) as a pair of equal
+// 16-bit values, when that is exact: c finite, a normal number of the
+// storage format, and no mantissa bits beyond the format's.  Returns false
+// otherwise (the kernel then keeps the FP32 factor for the whole item).
+template <int STORAGE>
+__device__ __forceinline__ bool pack_factor16(float c, uint32_t* packed) {
+  if constexpr (STORAGE == BP_STORAGE_F16) {
+    const float a = fabsf(c);
+    if (!(a >= 6.103515625e-05f && a <= 65504.0f)) return false;  // normal FP16
+    const __half h = __float2half_rn(c);
+    if (__half2float(h) != c) return false;
+    const uint32_t b = (uint32_t)__half_as_ushort(h);
+    *packed = b | (b << 16);
+    return true;
+  } else {
+    const float a = fabsf(c);
+    if (!(a >= FLT_MIN && a <= FLT_MAX)) return false;  // normal, finite
+    const uint32_t b = __float_as_uint(c);
+    if (b & 0xFFFFu) return false;
+    *packed = (b >> 16) | (b & 0xFFFF0000u);
+    return true;
+  }
+}
+
+// The staged shift-and-stack for one item (record, block tile, time tiles
+// [tau0, tau1)), shared by the plain and the persistent kernels.  A block
+// tile is one table tile (WS * KS == kTableTile) or a part of one: block
+// tile b covers sources (b % H) * K .. + K - 1 of table tile b / H.  A ring
+// stage carries SPS consecutive active stations (one mbarrier round trip per
+// SPS stations).
+template <int P, int KS, int MT, int WS, int NSTAGE, int SPS, bool MAXRED, bool CHECKED,
+          int STORAGE>
 struct Staged {
   static_assert(MT % 2 == 0 && KS % 2 == 0, "packed pairs");
   static_assert(!(CHECKED && STORAGE != BP_STORAGE_F32), "checked variant is FP32 only");
   using M = typename MetaT<P>::type;
   static constexpr bool F32 = STORAGE == BP_STORAGE_F32;
-  static constexpr int K = WS * KS;
+  static constexpr int K = WS * KS;   // sources per block
+  static_assert(kTableTile % K == 0, "a block covers a whole part of a table tile");
+  static constexpr int H = kTableTile / K;  // blocks per table tile
   static constexpr int TT = 32 * MT;
+  static_assert(TT <= kMaxTimeTile, "time tile beyond the trace layout's padding");
   static constexpr int NCONS = WS * 32;
   static constexpr int ESZ = F32 ? 4 : 2;  // bytes per stored element
   static constexpr int NVER = F32 ? 1 : kHalfCopies;  // stored copies per row
   static constexpr int RF = ring_row_factor<STORAGE>();
   static_assert(F32 || MT % 4 == 0, "16-bit lanes own runs of 4 samples");
+  // Samples per lane whose words are loaded before their arithmetic (the
+  // whole lane up to 16; longer lanes in groups of 16, to bound registers).
+  static constexpr int GS = MT > 16 ? 16 : MT;
+  static_assert(MT % GS == 0, "whole groups");
 
   struct Smem {
     unsigned char* ring;
@@ -365,6 +440,7 @@ struct Staged {
     unsigned long long* red;
     int4* srci;
     int* st_s;
+    int* st_j;
     int* st_lo;
     int* st_w;
     float* st_sc;
@@ -376,13 +452,14 @@ struct Staged {
   };
 
   __device__ static Smem carve(unsigned char* smem, int rowcap, int max_active) {
-    const WindowSmem<P, KS, MT, WS, NSTAGE, MAXRED> L(rowcap, max_active, RF);
+    const WindowSmem<P, KS, MT, WS, NSTAGE, SPS, MAXRED> L(rowcap, max_active, RF);
     Smem s;
     s.ring = smem + L.ring;
     s.meta_s = reinterpret_cast<M*>(smem + L.meta);
     s.red = reinterpret_cast<unsigned long long*>(smem + L.red);
     s.srci = reinterpret_cast<int4*>(smem + L.srci);
     s.st_s = reinterpret_cast<int*>(smem + L.st_s);
+    s.st_j = reinterpret_cast<int*>(smem + L.st_j);
     s.st_lo = reinterpret_cast<int*>(smem + L.st_lo);
     s.st_w = reinterpret_cast<int*>(smem + L.st_w);
     s.st_sc = reinterpret_cast<float*>(smem + L.st_sc);
@@ -408,12 +485,14 @@ struct Staged {
   // __syncthreads() between items.  `it0` is the block's stage counter
   // before the item; returns the number of stages the item used.
   __device__ static int run_item(const Smem& sm, const TableView& tb, const RecordView& rc,
-                                 int tile, int tau0, int tau1, int rowcap, int* status,
+                                 int btile, int tau0, int tau1, int rowcap, int* status,
                                  int it0) {
     const int tid = threadIdx.x;
     const int warp = tid >> 5;
     const int lane = tid & 31;
     const int row_words = rowcap * RF;  // one ring row (all copies) in 32-bit words
+    const int tile = btile / H;         // table tile
+    const int k0 = (btile - tile * H) * K;  // first source slot of this block in the tile
 
     // ---- prologue: the tile's stations (those the record uses) ----------
     if (warp == 0) {
@@ -428,37 +507,29 @@ struct Staged {
           use = !rc.station_mask || ((rc.station_mask[s >> 5] >> (s & 31)) & 1u);
         }
         const unsigned bal = __ballot_sync(0xFFFFFFFFu, use);
-        if (use) {
-          const int jj = n + __popc(bal & ((1u << lane) - 1u));
-          sm.st_s[jj] = j;  // table slot for now; station index filled below
-        }
+        if (use) sm.st_j[n + __popc(bal & ((1u << lane) - 1u))] = j;  // table slot
         n += __popc(bal);
       }
       if (lane == 0) *sm.n_act = n;
     }
     __syncthreads();
     const int n_active = *sm.n_act;
-    {
-      const M* gm = reinterpret_cast<const M*>(tb.meta) + (size_t)tile * tb.S * K;
-      const uint32_t copy_words = (uint32_t)rowcap >> 1;  // one 16-bit copy, in words
-      for (int i = tid; i < n_active * K; i += blockDim.x) {
-        const int jj = i / K, k = i - jj * K;
-        M m = gm[(size_t)sm.st_s[jj] * K + k];
-        if constexpr (!F32) {
-          // 16-bit: each sample offset becomes the (even) 32-bit word offset
-          // in the ring row of the copy that starts the run on an 8-byte
-          // boundary: 2 (off >> 2) + (off & 3) * rowcap / 2 (copy v starts
-          // v * rowcap / 2 words into the row).
-          auto wo = [&](uint32_t v) {
-            const uint32_t lo = v & 0xFFFFu, hi = v >> 16;
-            return (2 * (lo >> 2) + (lo & 3u) * copy_words) |
-                   ((2 * (hi >> 2) + (hi & 3u) * copy_words) << 16);
-          };
-          m.y = wo(m.y);
-          if constexpr (P > 2) m.z = wo(m.z);
-        }
-        sm.meta_s[i] = m;
+    // per active station: station index, scale, window starts and widths
+    for (int i = tid; i < n_active; i += blockDim.x) {
+      const int j = sm.st_j[i];
+      const int s = tb.st_s[(size_t)tile * tb.S + j];
+      sm.st_s[i] = s;
+      sm.st_sc[i] = F32 ? 1.0f : rc.scales[s];
+#pragma unroll
+      for (int p = 0; p < P; ++p) {
+        const size_t g = ((size_t)tile * tb.S + j) * P + p;
+        sm.st_lo[i * P + p] = tb.st_lo[g];
+        const int w = (int)align_up_sz((size_t)(TT + tb.st_spread[g] + 1), kAlign);
+        sm.st_w[i * P + p] = w;
+        if (w > rowcap) atomicOr(status, kStatusBadWindow);
       }
+    }
+    {
       // Per source slot: {source, first, end, 0} with [first, end) the
       // record-local samples the out-of-bounds rule keeps (strict: every
       // delay of the source inside the record, the lower bound in global
@@ -466,9 +537,10 @@ struct Staged {
       // beyond any sample index of a record.
       constexpr long long kFar = 1ll << 30;
       for (int i = tid; i < K; i += blockDim.x) {
-        int4 si = tb.src_info[(size_t)tile * K + i];
+        const size_t slot = (size_t)tile * kTableTile + k0 + i;
+        int4 si = tb.src_info[slot];
         if (rc.srcmm) {
-          const int2 mm = rc.srcmm[(size_t)tile * K + i];
+          const int2 mm = rc.srcmm[slot];
           si.y = mm.x;
           si.z = mm.y;
         }
@@ -483,25 +555,55 @@ struct Staged {
         sm.srci[i] = make_int4(si.x, (int)first, (int)end, 0);
       }
     }
-    __syncthreads();  // the meta copy above read st_s[] as table slots
-    for (int i = tid; i < n_active; i += blockDim.x) {
-      // entry i is read and rewritten by this thread only
-      const int j = sm.st_s[i];
-      const int s = tb.st_s[(size_t)tile * tb.S + j];
-      sm.st_s[i] = s;
-      sm.st_sc[i] = F32 ? 1.0f : rc.scales[s];
-#pragma unroll
-      for (int p = 0; p < P; ++p) {
-        const size_t g = ((size_t)tile * tb.S + j) * P + p;
-        sm.st_lo[i * P + p] = tb.st_lo[g];
-        const int w = (int)align_up_sz((size_t)(TT + tb.st_spread[g] + 1), kAlign);
-        sm.st_w[i * P + p] = w;
-        if (w > rowcap) atomicOr(status, kStatusBadWindow);
+    __syncthreads();
+    // Per (active station, source): weight and offsets.  16-bit storage: each
+    // sample offset becomes the (even) 32-bit word offset in the ring row of
+    // the copy that starts the run on an 8-byte boundary: 2 (off >> 2) +
+    // (off & 3) * rowcap / 2 (copy v starts v * rowcap / 2 words into the
+    // row); and when every factor c = w * scale of the item is exact in the
+    // 16-bit format, the weight word becomes c packed twice (0 for a zero
+    // weight) and the item runs the mixed-precision arithmetic.
+    bool fast16 = false;
+    {
+      const M* gm = reinterpret_cast<const M*>(tb.meta) + (size_t)tile * tb.S * kTableTile;
+      const uint32_t copy_words = (uint32_t)rowcap >> 1;  // one 16-bit copy, in words
+      int exact = 1;
+      for (int i = tid; i < n_active * K; i += blockDim.x) {
+        const int jj = i / K, k = i - jj * K;
+        M m = gm[(size_t)sm.st_j[jj] * kTableTile + k0 + k];
+        if constexpr (!F32) {
+          auto wo = [&](uint32_t v) {
+            const uint32_t lo = v & 0xFFFFu, hi = v >> 16;
+            return (2 * (lo >> 2) + (lo & 3u) * copy_words) |
+                   ((2 * (hi >> 2) + (hi & 3u) * copy_words) << 16);
+          };
+          m.y = wo(m.y);
+          if constexpr (P > 2) m.z = wo(m.z);
+          const float w = __uint_as_float(m.x);
+          uint32_t pk;
+          if (w != 0.0f && !pack_factor16<STORAGE>(w * sm.st_sc[jj], &pk)) exact = 0;
+        }
+        sm.meta_s[i] = m;
+      }
+      if constexpr (F32) {
+        __syncthreads();
+      } else {
+        fast16 = __syncthreads_and(exact) != 0;
+        if (fast16) {
+          for (int i = tid; i < n_active * K; i += blockDim.x) {
+            const int jj = i / K;
+            const float w = __uint_as_float(sm.meta_s[i].x);
+            uint32_t pk = 0u;
+            if (w != 0.0f) pack_factor16<STORAGE>(w * sm.st_sc[jj], &pk);
+            sm.meta_s[i].x = pk;
+          }
+          __syncthreads();
+        }
       }
     }
-    __syncthreads();
 
-    const int n_stages = (tau1 - tau0) * n_active;
+    const int n_grp = (n_active + SPS - 1) / SPS;  // stages per time tile
+    const int n_stages = (tau1 - tau0) * n_grp;
 
     // ---- producer warp ----------------------------------------------------
     if (warp == WS) {
@@ -514,39 +616,54 @@ struct Staged {
           if (it >= NSTAGE && !mbar_wait_bounded(&sm.empty[stage], ((it / NSTAGE) - 1) & 1,
                                                  sm.abort_flag, status))
             break;
-          const int tau = tau0 + r / n_active;
-          const int j = r - (r / n_active) * n_active;
+          const int tau = tau0 + r / n_grp;
+          const int j0 = (r - (r / n_grp) * n_grp) * SPS;
+          const int nj = min(SPS, n_active - j0);
           const int t0 = tau * TT;
-          const int s = sm.st_s[j];
-          // copy (p, v) reads trace row (s P + p) NVER + v, columns [col, col + w)
-          auto copy_ok = [&](int p) -> bool {
+          // copy (jj, p, v) reads trace row (s P + p) NVER + v, columns [col, col + w)
+          auto copy_ok = [&](int j, int p) -> bool {
 #if BP_DEBUG_CHECKS
+            const int s = sm.st_s[j];
             const int w = min(sm.st_w[j * P + p], rowcap);
             const long long col = (long long)rc.lpad + t0 + sm.st_lo[j * P + p];
             return s >= 0 && s < tb.S && w > 0 && col >= 0 && col + w <= rc.pitch &&
                    (col * ESZ) % 16 == 0 && ((long long)w * ESZ) % 16 == 0;
 #else
+            (void)j;
             (void)p;
             return true;
 #endif
           };
           uint32_t bytes = 0;
 #pragma unroll
-          for (int p = 0; p < P; ++p)
-            if (copy_ok(p)) bytes += (uint32_t)min(sm.st_w[j * P + p], rowcap) * ESZ * NVER;
-            else atomicOr(status, kStatusBadIndex);
+          for (int jj = 0; jj < SPS; ++jj) {
+            if (jj >= nj) break;
+#pragma unroll
+            for (int p = 0; p < P; ++p)
+              if (copy_ok(j0 + jj, p))
+                bytes += (uint32_t)min(sm.st_w[(j0 + jj) * P + p], rowcap) * ESZ * NVER;
+              else
+                atomicOr(status, kStatusBadIndex);
+          }
           mbar_arrive_expect_tx(&sm.full[stage], bytes);
 #pragma unroll
-          for (int p = 0; p < P; ++p) {
-            if (!copy_ok(p)) continue;
-            const int w = min(sm.st_w[j * P + p], rowcap);
-            const long long col = (long long)rc.lpad + t0 + sm.st_lo[j * P + p];
+          for (int jj = 0; jj < SPS; ++jj) {
+            if (jj >= nj) break;
+            const int j = j0 + jj;
+            const int s = sm.st_s[j];
 #pragma unroll
-            for (int v = 0; v < NVER; ++v) {
-              const size_t row = (size_t)(s * P + p) * NVER + v;
-              bulk_g2s(sm.ring + ((size_t)(stage * P + p) * row_words) * 4 +
-                           (size_t)v * rowcap * ESZ,
-                       tr + (row * rc.pitch + col) * ESZ, (uint32_t)w * ESZ, &sm.full[stage]);
+            for (int p = 0; p < P; ++p) {
+              if (!copy_ok(j, p)) continue;
+              const int w = min(sm.st_w[j * P + p], rowcap);
+              const long long col = (long long)rc.lpad + t0 + sm.st_lo[j * P + p];
+              unsigned char* dst =
+                  sm.ring + ((size_t)((stage * SPS + jj) * P + p) * row_words) * 4;
+#pragma unroll
+              for (int v = 0; v < NVER; ++v) {
+                const size_t row = (size_t)(s * P + p) * NVER + v;
+                bulk_g2s(dst + (size_t)v * rowcap * ESZ, tr + (row * rc.pitch + col) * ESZ,
+                         (uint32_t)w * ESZ, &sm.full[stage]);
+              }
             }
           }
           ++issued;
@@ -574,148 +691,23 @@ struct Staged {
         for (int m = 0; m < MT / 2; ++m) acc[k][m] = make_float2(0.0f, 0.0f);
       const int t0 = tau * TT;
 
-      for (int j = 0; j < n_active; ++j, ++it) {
+      for (int g = 0; g < n_grp; ++g, ++it) {
         const int stage = it % NSTAGE;
         mbar_wait_bounded(&sm.full[stage], (it / NSTAGE) & 1, sm.abort_flag, status);
-        // stage base in 32-bit words; row p of the stage at + p * rowcap words
-        const int sbase = stage * P * row_words;
-        const M* mrow = sm.meta_s + (size_t)j * K + warp * KS;
-        const float scale = sm.st_sc[j];
 #pragma unroll
-        for (int k2 = 0; k2 < KS; k2 += 2) {
-          M mm2[2];
-          if constexpr (P <= 2) {
-            // two sources' records in one 128-bit broadcast
-            const uint4 q4 = *reinterpret_cast<const uint4*>(mrow + k2);
-            mm2[0] = make_uint2(q4.x, q4.y);
-            mm2[1] = make_uint2(q4.z, q4.w);
-          } else {
-            mm2[0] = mrow[k2];
-            mm2[1] = mrow[k2 + 1];
-          }
-#pragma unroll
-          for (int h = 0; h < 2; ++h) {
-            const int k = k2 + h;
-            const M m = mm2[h];
-            const float w = __uint_as_float(m.x);
-            if (w == 0.0f) continue;  // warp-uniform: skipped station
-            if constexpr (!F32) {
-              // 16-bit: sum the phases, then one fused multiply-add per
-              // sample pair with c = w * scale (exact: scale is 2^k).
-              const float c = w * scale;
-              const float2 c2 = make_float2(c, c);
-              const uint2* src[P];  // word offsets prepared in the prologue (even)
-#pragma unroll
-              for (int p = 0; p < P; ++p)
-                src[p] = reinterpret_cast<const uint2*>(
-                             reinterpret_cast<const uint32_t*>(sm.ring) + sbase +
-                             p * row_words + meta_off<P>(m, p)) + lane;
-              uint32_t wd[P][MT / 2];  // all words first (see the FP32 path)
-#pragma unroll
-              for (int p = 0; p < P; ++p)
-#pragma unroll
-                for (int r = 0; r < MT / 4; ++r) {
-#if BP_DEBUG_CHECKS
-                  {  // the 4 samples of this load inside its copy's window
-                    const int copy_words = rowcap >> 1;
-                    const int wi = meta_off<P>(m, p) + 2 * lane + 64 * r;
-                    const int cv = wi / copy_words, pos = 2 * (wi - cv * copy_words);
-                    if (cv >= NVER || pos + 3 >= min(sm.st_w[j * P + p], rowcap)) {
-                      atomicOr(status, kStatusBadIndex);
-                      wd[p][2 * r] = wd[p][2 * r + 1] = 0u;
-                      continue;
-                    }
-                  }
-#endif
-                  const uint2 v = src[p][32 * r];  // samples 4 lane + 128 r + 0..3
-                  wd[p][2 * r] = v.x;
-                  wd[p][2 * r + 1] = v.y;
-                }
-#pragma unroll
-              for (int q = 0; q < MT / 2; ++q) {
-                float2 ps;
-                if constexpr (STORAGE == BP_STORAGE_F16) {
-                  // phases summed in FP16 pairs (one extra FP16 rounding of a
-                  // sum of values in [-P, P]), then widened once
-                  __half2 hs = *reinterpret_cast<const __half2*>(&wd[0][q]);
-#pragma unroll
-                  for (int p = 1; p < P; ++p)
-                    hs = __hadd2(hs, *reinterpret_cast<const __half2*>(&wd[p][q]));
-                  ps = __half22float2(hs);
-                } else {
-                  // BF16 -> FP32 is exact bit placement; phases summed in FP32
-                  ps = make_float2(__uint_as_float(wd[0][q] << 16),
-                                   __uint_as_float(wd[0][q] & 0xFFFF0000u));
-#pragma unroll
-                  for (int p = 1; p < P; ++p)
-                    ps = add2_rn(ps, make_float2(__uint_as_float(wd[p][q] << 16),
-                                                 __uint_as_float(wd[p][q] & 0xFFFF0000u)));
-                }
-                acc[k][q] = __ffma2_rn(c2, ps, acc[k][q]);
-              }
-            } else if constexpr (CHECKED) {
-#pragma unroll
-              for (int p = 0; p < P; ++p) {
-                const int off = meta_off<P>(m, p);
-                const float* src = reinterpret_cast<const float*>(sm.ring) + sbase +
-                                   p * row_words + off + lane;
-                const long long tb0 = (long long)t0 + lane + sm.st_lo[j * P + p] + off;
-#pragma unroll
-                for (int mm = 0; mm < MT; ++mm) {
-                  const long long tt = tb0 + 32 * mm;
-                  if (tt < 0 || tt >= rc.T) continue;
-#if BP_DEBUG_CHECKS
-                  if (off + lane + 32 * mm >= min(sm.st_w[j * P + p], rowcap)) {
-                    atomicOr(status, kStatusBadIndex);
-                    continue;
-                  }
-#endif
-                  const float v = __fadd_rn((mm & 1) ? acc[k][mm >> 1].y : acc[k][mm >> 1].x,
-                                            __fmul_rn(w, src[mm * 32]));
-                  if (mm & 1) acc[k][mm >> 1].y = v; else acc[k][mm >> 1].x = v;
-                }
-              }
-            } else {
-              // All of this source's words first, then the arithmetic: the
-              // loads of one (source, station) are independent, and issuing
-              // them together keeps P * MT shared-memory loads in flight.
-              const float* sbf = reinterpret_cast<const float*>(sm.ring) + sbase + lane;
-              float u[P][MT];
-#pragma unroll
-              for (int p = 0; p < P; ++p) {
-                const float* src = sbf + p * row_words + meta_off<P>(m, p);
-#pragma unroll
-                for (int mm = 0; mm < MT; ++mm) {
-#if BP_DEBUG_CHECKS
-                  if (meta_off<P>(m, p) + lane + 32 * mm >= min(sm.st_w[j * P + p], rowcap)) {
-                    atomicOr(status, kStatusBadIndex);
-                    u[p][mm] = 0.0f;
-                    continue;
-                  }
-#endif
-                  u[p][mm] = src[32 * mm];
-                }
-              }
-              if (w == 1.0f) {  // warp-uniform: 1 * u == u exactly, skip the multiply
-#pragma unroll
-                for (int p = 0; p < P; ++p)
-#pragma unroll
-                  for (int q = 0; q < MT / 2; ++q)
-                    acc[k][q] = add2_rn(acc[k][q], make_float2(u[p][2 * q], u[p][2 * q + 1]));
-              } else {
-                // Scalar rounded multiply then rounded add: a packed multiply
-                // followed by a packed add can be fused downstream, which would
-                // change the last bit against the reference.
-#pragma unroll
-                for (int p = 0; p < P; ++p)
-#pragma unroll
-                  for (int q = 0; q < MT / 2; ++q) {
-                    acc[k][q].x = __fadd_rn(acc[k][q].x, __fmul_rn(w, u[p][2 * q]));
-                    acc[k][q].y = __fadd_rn(acc[k][q].y, __fmul_rn(w, u[p][2 * q + 1]));
-                  }
-              }
-            }
-          }
+        for (int jj = 0; jj < SPS; ++jj) {
+          const int j = g * SPS + jj;
+          if (j >= n_active) break;
+          // station base in 32-bit words; row p at + p * row_words words
+          const int sbase = (stage * SPS + jj) * P * row_words;
+          const M* mrow = sm.meta_s + (size_t)j * K + warp * KS;
+          const float scale = sm.st_sc[j];
+          if (fast16)
+            station<true>(sm, rc, mrow, sbase, row_words, scale, j, t0, lane, rowcap, status,
+                          acc);
+          else
+            station<false>(sm, rc, mrow, sbase, row_words, scale, j, t0, lane, rowcap, status,
+                           acc);
         }
         __syncwarp();
         if (lane == 0) mbar_arrive(&sm.empty[stage]);
@@ -779,40 +771,220 @@ struct Staged {
     }
     return n_stages;
   }
+
+  // One active station j of the current stage for this warp's KS sources:
+  // acc[k][.] += w_k * (sum over phases of the station's shifted samples).
+  // FAST16 (16-bit storage, block-uniform): the weight words hold the packed
+  // 16-bit factors c = w * scale (see the prologue).
+  template <bool FAST16>
+  __device__ static __forceinline__ void station(const Smem& sm, const RecordView& rc,
+                                                 const M* mrow, int sbase, int row_words,
+                                                 float scale, int j, int t0, int lane,
+                                                 int rowcap, int* status,
+                                                 float2 (&acc)[KS][MT / 2]) {
+    (void)rc;
+    (void)j;
+    (void)t0;
+    (void)rowcap;
+    (void)status;
+    (void)scale;
+#pragma unroll
+    for (int k2 = 0; k2 < KS; k2 += 2) {
+      M mm2[2];
+      if constexpr (P <= 2) {
+        // two sources' records in one 128-bit broadcast
+        const uint4 q4 = *reinterpret_cast<const uint4*>(mrow + k2);
+        mm2[0] = make_uint2(q4.x, q4.y);
+        mm2[1] = make_uint2(q4.z, q4.w);
+      } else {
+        mm2[0] = mrow[k2];
+        mm2[1] = mrow[k2 + 1];
+      }
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int k = k2 + h;
+        const M m = mm2[h];
+        if constexpr (!F32) {
+          // FAST16: m.x is the packed 16-bit factor c (0: skipped station);
+          // otherwise m.x is the FP32 weight and c = w * scale (exact: scale
+          // is 2^k).  Both give the same value per sample: c times the phase
+          // sum (FP16: summed in half2 first; BF16: one product per phase)
+          // added to the FP32 accumulator with one rounding per product.
+          if (FAST16 ? (m.x == 0u) : (__uint_as_float(m.x) == 0.0f)) continue;  // warp-uniform
+          const float c = FAST16 ? 0.0f : __uint_as_float(m.x) * scale;
+          const float2 c2 = make_float2(c, c);
+          const uint2* src[P];  // word offsets prepared in the prologue (even)
+#pragma unroll
+          for (int p = 0; p < P; ++p)
+            src[p] = reinterpret_cast<const uint2*>(
+                         reinterpret_cast<const uint32_t*>(sm.ring) + sbase + p * row_words +
+                         meta_off<P>(m, p)) + lane;
+#pragma unroll
+          for (int g0 = 0; g0 < MT / 4; g0 += GS / 4) {
+            uint32_t wd[P][GS / 2];  // the group's words first
+#pragma unroll
+            for (int p = 0; p < P; ++p)
+#pragma unroll
+              for (int rr = 0; rr < GS / 4; ++rr) {
+                const int r = g0 + rr;
+#if BP_DEBUG_CHECKS
+                {  // the 4 samples of this load inside its copy's window
+                  const int copy_words = rowcap >> 1;
+                  const int wi = meta_off<P>(m, p) + 2 * lane + 64 * r;
+                  const int cv = wi / copy_words, pos = 2 * (wi - cv * copy_words);
+                  if (cv >= NVER || pos + 3 >= min(sm.st_w[j * P + p], rowcap)) {
+                    atomicOr(status, kStatusBadIndex);
+                    wd[p][2 * rr] = wd[p][2 * rr + 1] = 0u;
+                    continue;
+                  }
+                }
+#endif
+                const uint2 v = src[p][32 * r];  // samples 4 lane + 128 r + 0..3
+                wd[p][2 * rr] = v.x;
+                wd[p][2 * rr + 1] = v.y;
+              }
+#pragma unroll
+            for (int qq = 0; qq < GS / 2; ++qq) {
+              const int q = 2 * g0 + qq;
+              if constexpr (STORAGE == BP_STORAGE_F16) {
+                // phases summed in FP16 pairs (one extra FP16 rounding of a
+                // sum of values in [-P, P])
+                uint32_t hs = wd[0][qq];
+#pragma unroll
+                for (int p = 1; p < P; ++p) hs = hadd2_rn(hs, wd[p][qq]);
+                if constexpr (FAST16) {
+                  fma2_f32_f16(acc[k][q], hs, m.x);
+                } else {
+                  __half2 hh;
+                  memcpy(&hh, &hs, 4);
+                  acc[k][q] = __ffma2_rn(c2, __half22float2(hh), acc[k][q]);
+                }
+              } else {
+                // BF16: one FMA per phase and sample, phases ascending
+#pragma unroll
+                for (int p = 0; p < P; ++p) {
+                  if constexpr (FAST16) {
+                    fma2_f32_bf16(acc[k][q], wd[p][qq], m.x);
+                  } else {
+                    const float2 u = make_float2(__uint_as_float(wd[p][qq] << 16),
+                                                 __uint_as_float(wd[p][qq] & 0xFFFF0000u));
+                    acc[k][q] = __ffma2_rn(c2, u, acc[k][q]);
+                  }
+                }
+              }
+            }
+          }
+        } else if constexpr (CHECKED) {
+          const float w = __uint_as_float(m.x);
+          if (w == 0.0f) continue;  // warp-uniform: skipped station
+#pragma unroll
+          for (int p = 0; p < P; ++p) {
+            const int off = meta_off<P>(m, p);
+            const float* src = reinterpret_cast<const float*>(sm.ring) + sbase +
+                               p * row_words + off + lane;
+            const long long tb0 = (long long)t0 + lane + sm.st_lo[j * P + p] + off;
+#pragma unroll
+            for (int mm = 0; mm < MT; ++mm) {
+              const long long tt = tb0 + 32 * mm;
+              if (tt < 0 || tt >= rc.T) continue;
+#if BP_DEBUG_CHECKS
+              if (off + lane + 32 * mm >= min(sm.st_w[j * P + p], rowcap)) {
+                atomicOr(status, kStatusBadIndex);
+                continue;
+              }
+#endif
+              const float v = __fadd_rn((mm & 1) ? acc[k][mm >> 1].y : acc[k][mm >> 1].x,
+                                        __fmul_rn(w, src[mm * 32]));
+              if (mm & 1) acc[k][mm >> 1].y = v; else acc[k][mm >> 1].x = v;
+            }
+          }
+        } else {
+          const float w = __uint_as_float(m.x);
+          if (w == 0.0f) continue;  // warp-uniform: skipped station
+          // All of this source's words of a group first, then the arithmetic:
+          // the loads of one (source, station) are independent, and issuing
+          // them together keeps P * GS shared-memory loads in flight.
+          const float* sbf = reinterpret_cast<const float*>(sm.ring) + sbase + lane;
+#pragma unroll
+          for (int g0 = 0; g0 < MT; g0 += GS) {
+            float u[P][GS];
+#pragma unroll
+            for (int p = 0; p < P; ++p) {
+              const float* src = sbf + p * row_words + meta_off<P>(m, p);
+#pragma unroll
+              for (int mm = 0; mm < GS; ++mm) {
+#if BP_DEBUG_CHECKS
+                if (meta_off<P>(m, p) + lane + 32 * (g0 + mm) >=
+                    min(sm.st_w[j * P + p], rowcap)) {
+                  atomicOr(status, kStatusBadIndex);
+                  u[p][mm] = 0.0f;
+                  continue;
+                }
+#endif
+                u[p][mm] = src[32 * (g0 + mm)];
+              }
+            }
+            if (w == 1.0f) {  // warp-uniform: 1 * u == u exactly, skip the multiply
+#pragma unroll
+              for (int p = 0; p < P; ++p)
+#pragma unroll
+                for (int qq = 0; qq < GS / 2; ++qq) {
+                  const int q = g0 / 2 + qq;
+                  acc[k][q] = add2_rn(acc[k][q], make_float2(u[p][2 * qq], u[p][2 * qq + 1]));
+                }
+            } else {
+              // Scalar rounded multiply then rounded add: a packed multiply
+              // followed by a packed add can be fused downstream, which would
+              // change the last bit against the reference.
+#pragma unroll
+              for (int p = 0; p < P; ++p)
+#pragma unroll
+                for (int qq = 0; qq < GS / 2; ++qq) {
+                  const int q = g0 / 2 + qq;
+                  acc[k][q].x = __fadd_rn(acc[k][q].x, __fmul_rn(w, u[p][2 * qq]));
+                  acc[k][q].y = __fadd_rn(acc[k][q].y, __fmul_rn(w, u[p][2 * qq + 1]));
+                }
+            }
+          }
+        }
+      }
+    }
+  }
 };
 
-// Plain launch: one record, block = (source tile, chunk of time tiles),
+// Plain launch: one record, block = (block tile, chunk of time tiles),
 // time-chunk major so that the blocks in flight share an L2-resident stretch
 // of trace.
-template <int P, int KS, int MT, int WS, int NSTAGE, int MINB, bool MAXRED, bool CHECKED,
-          int STORAGE>
+template <int P, int KS, int MT, int WS, int NSTAGE, int SPS, int MINB, bool MAXRED,
+          bool CHECKED, int STORAGE>
 __global__ void __launch_bounds__((WS + 1) * 32, MINB)
 beam_window_kernel(const LaunchArgs a) {
-  using St = Staged<P, KS, MT, WS, NSTAGE, MAXRED, CHECKED, STORAGE>;
+  using St = Staged<P, KS, MT, WS, NSTAGE, SPS, MAXRED, CHECKED, STORAGE>;
   extern __shared__ __align__(128) unsigned char smem[];
   const typename St::Smem sm = St::carve(smem, a.rowcap, a.max_active);
   if (threadIdx.x == 0) St::init_barriers(sm);
   __syncthreads();
-  const int tile = blockIdx.x % a.tab0.n_tiles;
-  const int chunk = blockIdx.x / a.tab0.n_tiles;
+  const int n_btiles = a.tab0.n_tiles * St::H;
+  const int btile = blockIdx.x % n_btiles;
+  const int chunk = blockIdx.x / n_btiles;
   const int tau_first = a.rec0.out0 / St::TT;
   const int tau_end = (a.rec0.out1 + St::TT - 1) / St::TT;
   const int tau0 = tau_first + chunk * a.tiles_per_chunk;
   const int tau1 = min(tau0 + a.tiles_per_chunk, tau_end);
-  St::run_item(sm, a.tab0, a.rec0, tile, tau0, tau1, a.rowcap, a.status, 0);
+  St::run_item(sm, a.tab0, a.rec0, btile, tau0, tau1, a.rowcap, a.status, 0);
 }
 
 // Persistent launch: a fixed grid whose blocks pop work items from a device
 // queue until it is empty.  The queue is a counter over the items of all
 // records (record r owns items rec_prefix[r] .. rec_prefix[r + 1] - 1, each a
-// source tile x a chunk of r.tpc time tiles, time-chunk major).  Records may
+// block tile x a chunk of r.tpc time tiles, time-chunk major).  Records may
 // differ in length, station subset and table; storage, phases and reduce are
 // the launch's.
-template <int P, int KS, int MT, int WS, int NSTAGE, int MINB, bool MAXRED, bool CHECKED,
-          int STORAGE>
+template <int P, int KS, int MT, int WS, int NSTAGE, int SPS, int MINB, bool MAXRED,
+          bool CHECKED, int STORAGE>
 __global__ void __launch_bounds__((WS + 1) * 32, MINB)
 beam_batch_kernel(const LaunchArgs a) {
-  using St = Staged<P, KS, MT, WS, NSTAGE, MAXRED, CHECKED, STORAGE>;
+  using St = Staged<P, KS, MT, WS, NSTAGE, SPS, MAXRED, CHECKED, STORAGE>;
   extern __shared__ __align__(128) unsigned char smem[];
   const typename St::Smem sm = St::carve(smem, a.rowcap, a.max_active);
   if (threadIdx.x == 0) St::init_barriers(sm);
@@ -831,14 +1003,14 @@ beam_batch_kernel(const LaunchArgs a) {
           if (a.rec_prefix[mid] <= i) lo = mid; else hi = mid - 1;
         }
         const RecordView& r = a.records[lo];
-        const int n_tiles = a.tables[r.table].n_tiles;
+        const int n_btiles = a.tables[r.table].n_tiles * St::H;
         const long long local = i - a.rec_prefix[lo];
-        const int chunk = (int)(local / n_tiles);
-        const int tile = (int)(local - (long long)chunk * n_tiles);
+        const int chunk = (int)(local / n_btiles);
+        const int btile = (int)(local - (long long)chunk * n_btiles);
         const int tau_first = r.out0 / St::TT;
         const int tau_end = (r.out1 + St::TT - 1) / St::TT;
         const int tau0 = tau_first + chunk * r.tpc;
-        cur = make_int4(lo, tile, tau0, min(tau0 + r.tpc, tau_end));
+        cur = make_int4(lo, btile, tau0, min(tau0 + r.tpc, tau_end));
       }
       *sm.cur_item = cur;
     }

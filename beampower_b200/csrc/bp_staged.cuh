@@ -13,14 +13,14 @@ template <int CFG, int P, bool MAXRED, bool CHECKED, int STORAGE>
 int launch_window_p(const bp::LaunchArgs& a, bool batch, long long plain_blocks, int dev,
                     cudaStream_t st) {
   using C = KCfg<CFG>;
-  using L = bp::WindowSmem<P, C::KS, C::MT, C::WS, C::NSTAGE, MAXRED>;
+  using L = bp::WindowSmem<P, C::KS, C::MT, C::WS, C::NSTAGE, C::SPS, MAXRED>;
   const L lay(a.rowcap, a.max_active, bp::ring_row_factor<STORAGE>());
   if (lay.total > (size_t)device_smem_optin(dev))
     return fail(BP_ERR_UNSUPPORTED, "staged kernel needs %zu B of shared memory", lay.total);
   constexpr int threads = bp::WindowCfg<P, C::KS, C::MT, C::WS>::kThreads;
   if (batch) {
-    auto kern = bp::beam_batch_kernel<P, C::KS, C::MT, C::WS, C::NSTAGE, C::MINB, MAXRED,
-                                      CHECKED, STORAGE>;
+    auto kern = bp::beam_batch_kernel<P, C::KS, C::MT, C::WS, C::NSTAGE, C::SPS, C::MINB,
+                                      MAXRED, CHECKED, STORAGE>;
     BP_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)lay.total));
     int per_sm = 0;
@@ -29,8 +29,8 @@ int launch_window_p(const bp::LaunchArgs& a, bool batch, long long plain_blocks,
     kern<<<grid, threads, lay.total, st>>>(a);
     BP_LAUNCHED("beam_batch_kernel");
   } else {
-    auto kern = bp::beam_window_kernel<P, C::KS, C::MT, C::WS, C::NSTAGE, C::MINB, MAXRED,
-                                       CHECKED, STORAGE>;
+    auto kern = bp::beam_window_kernel<P, C::KS, C::MT, C::WS, C::NSTAGE, C::SPS, C::MINB,
+                                       MAXRED, CHECKED, STORAGE>;
     BP_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)lay.total));
     if (plain_blocks > kMaxInt) return fail(BP_ERR_UNSUPPORTED, "grid too large");

@@ -432,16 +432,24 @@ BP_API int bp_keys_from_shared_dev(const unsigned long long *d_keys, size_t n_sa
 
 /* ---- staged-kernel configurations (autotuning) -------------------------- */
 /* The staged kernel exists in several shapes (sources per thread, samples per
- * lane, consumer warps, ring stages), all over the same 64-source tables.
+ * lane, consumer warps, ring stages, stations per ring stage, sources per
+ * block, blocks per SM), all over the same 64-source tables.
  * bp_set_kernel_config chooses one per (storage, reduce) for every later
  * launch in the process (-1: built-in default); the environment variable
  * BEAMPOWER_B200_KERNEL_CONFIG overrides it.  beampower_b200/autotune.py
- * times the shapes on a workload and stores its choices.  No reference
- * counterpart (the reference has one launch shape, beamform.cu:10). */
+ * times the shapes on a workload and stores its choices.  A shape whose
+ * shared memory does not fit a table falls back to config 0 for that table.
+ * No reference counterpart (the reference has one launch shape,
+ * beamform.cu:10). */
 BP_API int bp_kernel_config_count(void);
 BP_API int bp_kernel_config_describe(int config, int *sources_per_thread,
                                      int *samples_per_lane, int *consumer_warps,
                                      int *stages);
+/* The other dimensions of a shape: stations carried by one ring stage (one
+ * mbarrier round trip each), sources per block (64: one block per table tile;
+ * 32: two blocks share a tile) and the blocks per SM it is built for. */
+BP_API int bp_kernel_config_shape(int config, int *stations_per_stage,
+                                  int *sources_per_block, int *blocks_per_sm);
 BP_API int bp_set_kernel_config(int storage, int reduce, int config);
 BP_API int bp_get_kernel_config(int storage, int reduce);
 

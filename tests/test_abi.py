@@ -120,7 +120,10 @@ def test_key_order_matches_reference_max_rule():
 def test_kernel_configs_described():
     from beampower_b200.autotune import configs
     cfgs = configs()
-    assert len(cfgs) >= 2
+    assert len(cfgs) >= 6
     for c, d in cfgs:
-        assert d["sources_per_thread"] * d["consumer_warps"] == 64  # the table's tile
+        # one block per 64-source table tile, or blocks sharing a tile
+        assert d["sources_per_thread"] * d["consumer_warps"] == d["sources_per_block"]
+        assert 64 % d["sources_per_block"] == 0
         assert d["samples_per_lane"] % 2 == 0 and d["stages"] >= 2
+        assert d["stations_per_stage"] in (1, 2) and d["blocks_per_sm"] >= 1
