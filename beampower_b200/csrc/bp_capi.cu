@@ -89,7 +89,8 @@ constexpr CfgDesc cfg_desc() {
   return {C::KS, C::MT, C::WS, C::NSTAGE, C::SPS, C::K, C::MINB};
 }
 constexpr CfgDesc kCfgDesc[kNumConfigs] = {cfg_desc<0>(), cfg_desc<1>(), cfg_desc<2>(),
-                                           cfg_desc<3>(), cfg_desc<4>(), cfg_desc<5>()};
+                                           cfg_desc<3>(), cfg_desc<4>(), cfg_desc<5>(),
+                                           cfg_desc<6>(), cfg_desc<7>()};
 
 inline const CfgDesc& cfg_of(int cfg) {
   return kCfgDesc[(cfg >= 0 && cfg < kNumConfigs) ? cfg : 0];
@@ -279,6 +280,8 @@ int launch_window(int cfg, int P, bool checked, int storage, const bp::LaunchArg
     case 3: return launch_window_c<3, MAXRED>(P, checked, storage, a, batch, blocks, dev, st);
     case 4: return launch_window_c<4, MAXRED>(P, checked, storage, a, batch, blocks, dev, st);
     case 5: return launch_window_c<5, MAXRED>(P, checked, storage, a, batch, blocks, dev, st);
+    case 6: return launch_window_c<6, MAXRED>(P, checked, storage, a, batch, blocks, dev, st);
+    case 7: return launch_window_c<7, MAXRED>(P, checked, storage, a, batch, blocks, dev, st);
     default: return launch_window_c<0, MAXRED>(P, checked, storage, a, batch, blocks, dev, st);
   }
 }
@@ -315,6 +318,8 @@ size_t staged_smem_bytes(int cfg, int P, bool maxred, int rowcap, int max_active
     case 3: return staged_smem_cfg<3>(P, maxred, rowcap, max_active, rf);
     case 4: return staged_smem_cfg<4>(P, maxred, rowcap, max_active, rf);
     case 5: return staged_smem_cfg<5>(P, maxred, rowcap, max_active, rf);
+    case 6: return staged_smem_cfg<6>(P, maxred, rowcap, max_active, rf);
+    case 7: return staged_smem_cfg<7>(P, maxred, rowcap, max_active, rf);
     default: return staged_smem_cfg<0>(P, maxred, rowcap, max_active, rf);
   }
 }
@@ -609,6 +614,11 @@ int bp_table_create(const int32_t* d_delays, const float* d_weights, size_t N, s
     rc = build_tiling_map(d_delays, d_weights, N, S, P, K, (int)n_tiles,
                           const_cast<int*>(t->dev.perm), st);
     if (rc) return bail(rc);
+    bp::sort_tile_slots_kernel<<<(unsigned)n_tiles, bp::kTableTile, 0, st>>>(
+        const_cast<int*>(t->dev.perm), (int)N);
+    g_launches.fetch_add(1);
+    if (cudaError_t le = cudaGetLastError(); le != cudaSuccess)
+      return bail(cuda_fail(le, "launch sort_tile_slots_kernel"));
     switch (P) {
       case 1: rc = launch_table_build<1>(d_delays, d_weights, t->dev, st); break;
       case 2: rc = launch_table_build<2>(d_delays, d_weights, t->dev, st); break;

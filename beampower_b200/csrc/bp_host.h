@@ -50,6 +50,11 @@ constexpr long long kMaxInt = std::numeric_limits<int>::max();
 //   0: 8 x 8, MT 8,  SPS 1, 2/SM     1: 16 x 4, MT 16, SPS 1, 1/SM
 //   2: 16 x 4, MT 16, SPS 2, 1/SM    3: 8 x 8, MT 8,  SPS 2, 2/SM
 //   4: 16 x 2, MT 32, SPS 1, 1/SM    5: 16 x 2, MT 32, SPS 2, 1/SM
+//   6: 8 x 8, MT 16, SPS 2, 1/SM     7: 8 x 8, MT 16, SPS 1, 1/SM
+// Registers: a sub-partition holds 16K; 17 warps (16 consumers + producer)
+// or 2 x 9 warps put 5 warps on one sub-partition and cap a thread at 96
+// registers, 9 warps at one block per SM allow 168 (configs 6 and 7: 8 x 16
+// accumulators per thread).
 // (A shape of 16 warps x 4 sources x 8 samples at 2 blocks per SM was
 // measured slower for every storage type: capped at 56 registers it spills.)
 #ifndef BP_NSTAGE
@@ -68,7 +73,9 @@ template <> struct KCfg<2> : KShape<16, 4, 16, 2, 1> {};
 template <> struct KCfg<3> : KShape<8, 8, 8, 2, 2> {};
 template <> struct KCfg<4> : KShape<16, 2, 32, 1, 1> {};
 template <> struct KCfg<5> : KShape<16, 2, 32, 2, 1> {};
-constexpr int kNumConfigs = 6;
+template <> struct KCfg<6> : KShape<8, 8, 16, 2, 1> {};
+template <> struct KCfg<7> : KShape<8, 8, 16, 1, 1> {};
+constexpr int kNumConfigs = 8;
 constexpr int kTileSources = bp::kTableTile;
 
 // Launches the staged kernel of config CFG (plain grid of `blocks` blocks, or
@@ -89,6 +96,8 @@ BP_EXTERN_CFG(2)
 BP_EXTERN_CFG(3)
 BP_EXTERN_CFG(4)
 BP_EXTERN_CFG(5)
+BP_EXTERN_CFG(6)
+BP_EXTERN_CFG(7)
 #undef BP_EXTERN_CFG
 
 }  // namespace bp_host

@@ -308,6 +308,14 @@ struct WindowCfg {
 
 __host__ __device__ inline size_t align_up_sz(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
+// Rows of the cross-warp max buffer: one per consumer warp (plain stores,
+// then a max over the rows), or, where that would take more than 64 KB, one
+// row that the warps max into with shared-memory atomics.
+template <int WS, int TT>
+__host__ __device__ constexpr int red_rows() {
+  return (size_t)WS * TT * sizeof(unsigned long long) > 65536 ? 1 : WS;
+}
+
 // Shared-memory carve-up, used identically by host (size) and device.  A
 // ring row holds `rowcap` FP32 elements, or `rowcap` 16-bit elements of
 // each of the kHalfCopies copies; a stage holds SPS stations x P rows.
@@ -325,7 +333,7 @@ struct WindowSmem {
     o = align_up_sz(o, 16);
     meta = o;        o += (size_t)max_active * K * sizeof(M);
     o = align_up_sz(o, 16);
-    red = o;         o += MAXRED ? (size_t)WS * TT * sizeof(unsigned long long) : 0;
+    red = o;         o += MAXRED ? (size_t)red_rows<WS, TT>() * TT * sizeof(unsigned long long) : 0;
     o = align_up_sz(o, 16);
     srci = o;        o += (size_t)K * sizeof(int4);
     st_s = o;        o += (size_t)max_active * sizeof(int);
@@ -529,6 +537,8 @@ struct Staged {
         if (w > rowcap) atomicOr(status, kStatusBadWindow);
       }
     }
+    if constexpr (MAXRED && red_rows<WS, TT>() == 1)
+      for (int i = tid; i < TT; i += blockDim.x) sm.red[i] = 0ull;
     {
       // Per source slot: {source, first, end, 0} with [first, end) the
       // record-local samples the out-of-bounds rule keeps (strict: every
@@ -557,10 +567,10 @@ struct Staged {
     }
     __syncthreads();
     // Per (active station, source): weight and offsets.  16-bit storage: each
-    // sample offset becomes the (even) 32-bit word offset in the ring row of
-    // the copy that starts the run on an 8-byte boundary: 2 (off >> 2) +
-    // (off & 3) * rowcap / 2 (copy v starts v * rowcap / 2 words into the
-    // row); and when every factor c = w * scale of the item is exact in the
+    // sample offset becomes the byte offset in the ring row of the copy that
+    // starts the run on an 8-byte boundary: 4 (2 (off >> 2) + (off & 3) *
+    // rowcap / 2) (copy v starts v * rowcap / 2 words into the row; the host
+    // keeps 8 rowcap below 2^16); and when every factor c = w * scale of the item is exact in the
     // 16-bit format, the weight word becomes c packed twice (0 for a zero
     // weight) and the item runs the mixed-precision arithmetic.
     bool fast16 = false;
@@ -574,8 +584,8 @@ struct Staged {
         if constexpr (!F32) {
           auto wo = [&](uint32_t v) {
             const uint32_t lo = v & 0xFFFFu, hi = v >> 16;
-            return (2 * (lo >> 2) + (lo & 3u) * copy_words) |
-                   ((2 * (hi >> 2) + (hi & 3u) * copy_words) << 16);
+            return (4 * (2 * (lo >> 2) + (lo & 3u) * copy_words)) |
+                   ((4 * (2 * (hi >> 2) + (hi & 3u) * copy_words)) << 16);
           };
           m.y = wo(m.y);
           if constexpr (P > 2) m.z = wo(m.z);
@@ -681,6 +691,25 @@ struct Staged {
     }
 
     // ---- consumer warps ---------------------------------------------------
+    if constexpr (F32) {
+      consume<false>(sm, rc, tau0, tau1, n_active, n_grp, rowcap, status, it0);
+    } else {
+      if (fast16) consume<true>(sm, rc, tau0, tau1, n_active, n_grp, rowcap, status, it0);
+      else consume<false>(sm, rc, tau0, tau1, n_active, n_grp, rowcap, status, it0);
+    }
+    return n_stages;
+  }
+
+  // The consumer warps' part of an item: for every time tile, the stages'
+  // stations into the accumulators, then the epilogue.  FAST16: the item's
+  // weight words hold packed 16-bit factors (block-uniform choice).
+  template <bool FAST16>
+  __device__ static void consume(const Smem& sm, const RecordView& rc, int tau0, int tau1,
+                                 int n_active, int n_grp, int rowcap, int* status, int it0) {
+    const int tid = threadIdx.x;
+    const int warp = tid >> 5;
+    const int lane = tid & 31;
+    const int row_words = rowcap * RF;
     const int4* my_src = sm.srci + warp * KS;
     int it = it0;
     for (int tau = tau0; tau < tau1; ++tau) {
@@ -701,13 +730,8 @@ struct Staged {
           // station base in 32-bit words; row p at + p * row_words words
           const int sbase = (stage * SPS + jj) * P * row_words;
           const M* mrow = sm.meta_s + (size_t)j * K + warp * KS;
-          const float scale = sm.st_sc[j];
-          if (fast16)
-            station<true>(sm, rc, mrow, sbase, row_words, scale, j, t0, lane, rowcap, status,
-                          acc);
-          else
-            station<false>(sm, rc, mrow, sbase, row_words, scale, j, t0, lane, rowcap, status,
-                           acc);
+          station<FAST16>(sm, rc, mrow, sbase, row_words, sm.st_sc[j], j, t0, lane, rowcap,
+                          status, acc);
         }
         __syncwarp();
         if (lane == 0) mbar_arrive(&sm.empty[stage]);
@@ -715,40 +739,81 @@ struct Staged {
 
       // ---- epilogue of the time tile ----
       if constexpr (MAXRED) {
-        // source-major: each slot read once; the best key per sample stays in
-        // registers while the accumulators of processed sources die
-        unsigned long long best[MT / 2][2];
+        // Per sample, the thread's best (value, source) over its KS slots.
+        // The table orders each tile's slots by source index, so ascending
+        // slots are ascending sources and a strict `>` keeps the lowest
+        // index among equal maxima; seeding with -FLT_MAX makes NaN and
+        // -FLT_MAX (and below) lose, as in the reference's running max.
+        float bv[MT / 2][2];
+        int bi[MT / 2][2];
 #pragma unroll
-        for (int q = 0; q < MT / 2; ++q) best[q][0] = best[q][1] = 0ull;
+        for (int q = 0; q < MT / 2; ++q)
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            bv[q][h] = -FLT_MAX;
+            bi[q][h] = -1;
+          }
 #pragma unroll
         for (int k = 0; k < KS; ++k) {
           const int4 si = my_src[k];
+          if (si.y <= t0 && t0 + TT <= si.z) {  // warp-uniform: the whole tile is kept
 #pragma unroll
-          for (int q = 0; q < MT / 2; ++q) {
+            for (int q = 0; q < MT / 2; ++q)
 #pragma unroll
-            for (int h = 0; h < 2; ++h) {
-              const int t = t0 + pair_sample<STORAGE>(lane, q, h);
-              if (t < si.y || t >= si.z) continue;  // outside the kept samples (or no source)
-              const unsigned long long key = make_key(h ? acc[k][q].y : acc[k][q].x, si.x);
-              best[q][h] = key > best[q][h] ? key : best[q][h];
-            }
+              for (int h = 0; h < 2; ++h) {
+                const float v = h ? acc[k][q].y : acc[k][q].x;
+                if (v > bv[q][h]) {
+                  bv[q][h] = v;
+                  bi[q][h] = si.x;
+                }
+              }
+          } else {
+#pragma unroll
+            for (int q = 0; q < MT / 2; ++q)
+#pragma unroll
+              for (int h = 0; h < 2; ++h) {
+                const int t = t0 + pair_sample<STORAGE>(lane, q, h);
+                if (t < si.y || t >= si.z) continue;  // outside the kept samples (or no source)
+                const float v = h ? acc[k][q].y : acc[k][q].x;
+                if (v > bv[q][h]) {
+                  bv[q][h] = v;
+                  bi[q][h] = si.x;
+                }
+              }
           }
         }
+        unsigned long long best[MT / 2][2];
 #pragma unroll
         for (int q = 0; q < MT / 2; ++q)
 #pragma unroll
           for (int h = 0; h < 2; ++h)
-            sm.red[warp * TT + pair_sample<STORAGE>(lane, q, h)] = best[q][h];
+            best[q][h] = bi[q][h] >= 0 ? make_key(bv[q][h], bi[q][h]) : 0ull;
+        constexpr int kRows = red_rows<WS, TT>();
+        if constexpr (kRows == WS) {
+#pragma unroll
+          for (int q = 0; q < MT / 2; ++q)
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
+              sm.red[warp * TT + pair_sample<STORAGE>(lane, q, h)] = best[q][h];
+        } else {
+          // one shared row (zero on entry): max of the warps' keys
+#pragma unroll
+          for (int q = 0; q < MT / 2; ++q)
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
+              if (best[q][h]) atomicMax(&sm.red[pair_sample<STORAGE>(lane, q, h)], best[q][h]);
+        }
         named_barrier_sync(1, NCONS);
         for (int i = tid; i < TT; i += NCONS) {
-          unsigned long long best = 0ull;
+          unsigned long long b = 0ull;
 #pragma unroll
-          for (int w = 0; w < WS; ++w) {
+          for (int w = 0; w < kRows; ++w) {
             const unsigned long long v = sm.red[w * TT + i];
-            best = v > best ? v : best;
+            b = v > b ? v : b;
           }
+          if constexpr (kRows == 1) sm.red[i] = 0ull;  // zero again for the next tile
           const int t = t0 + i;
-          if (best != 0ull && t >= rc.out0 && t < rc.out1) red_max_u64(&rc.keys[t - rc.out0], best);
+          if (b != 0ull && t >= rc.out0 && t < rc.out1) red_max_u64(&rc.keys[t - rc.out0], b);
         }
         named_barrier_sync(1, NCONS);
       } else {
@@ -769,7 +834,6 @@ struct Staged {
         }
       }
     }
-    return n_stages;
   }
 
   // One active station j of the current stage for this warp's KS sources:
@@ -813,12 +877,12 @@ struct Staged {
           if (FAST16 ? (m.x == 0u) : (__uint_as_float(m.x) == 0.0f)) continue;  // warp-uniform
           const float c = FAST16 ? 0.0f : __uint_as_float(m.x) * scale;
           const float2 c2 = make_float2(c, c);
-          const uint2* src[P];  // word offsets prepared in the prologue (even)
+          const uint2* src[P];  // byte offsets prepared in the prologue (multiples of 8)
 #pragma unroll
           for (int p = 0; p < P; ++p)
             src[p] = reinterpret_cast<const uint2*>(
-                         reinterpret_cast<const uint32_t*>(sm.ring) + sbase + p * row_words +
-                         meta_off<P>(m, p)) + lane;
+                         sm.ring + (size_t)(sbase + p * row_words) * 4 + meta_off<P>(m, p)) +
+                     lane;
 #pragma unroll
           for (int g0 = 0; g0 < MT / 4; g0 += GS / 4) {
             uint32_t wd[P][GS / 2];  // the group's words first
@@ -830,7 +894,7 @@ struct Staged {
 #if BP_DEBUG_CHECKS
                 {  // the 4 samples of this load inside its copy's window
                   const int copy_words = rowcap >> 1;
-                  const int wi = meta_off<P>(m, p) + 2 * lane + 64 * r;
+                  const int wi = meta_off<P>(m, p) / 4 + 2 * lane + 64 * r;
                   const int cv = wi / copy_words, pos = 2 * (wi - cv * copy_words);
                   if (cv >= NVER || pos + 3 >= min(sm.st_w[j * P + p], rowcap)) {
                     atomicOr(status, kStatusBadIndex);
@@ -1356,6 +1420,23 @@ __global__ void split_keys_kernel(const int32_t* __restrict__ delays, int D, int
 __global__ void iota_perm_kernel(int* __restrict__ perm, int N, int total) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < total) perm[i] = (i < N) ? i : -1;
+}
+
+// Orders the slots of every tile by source index (unused slots last), so
+// that ascending slots are ascending sources: the staged kernel's epilogue
+// then keeps the lowest source index among equal maxima with a plain `>`.
+// One block of kTableTile threads per tile.
+__global__ void sort_tile_slots_kernel(int* __restrict__ perm, int N) {
+  __shared__ int v[kTableTile];
+  const int k = threadIdx.x;
+  const size_t base = (size_t)blockIdx.x * kTableTile;
+  const int o = perm[base + k];
+  v[k] = (o >= 0 && o < N) ? o : INT_MAX;
+  __syncthreads();
+  const int mine = v[k];
+  int rank = 0;
+  for (int j = 0; j < kTableTile; ++j) rank += (v[j] < mine) || (v[j] == mine && j < k);
+  perm[base + rank] = mine == INT_MAX ? -1 : mine;
 }
 
 // ---------------------------------------------------------------------------

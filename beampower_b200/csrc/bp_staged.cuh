@@ -17,6 +17,10 @@ int launch_window_p(const bp::LaunchArgs& a, bool batch, long long plain_blocks,
   const L lay(a.rowcap, a.max_active, bp::ring_row_factor<STORAGE>());
   if (lay.total > (size_t)device_smem_optin(dev))
     return fail(BP_ERR_UNSUPPORTED, "staged kernel needs %zu B of shared memory", lay.total);
+  // 16-bit storage addresses ring rows with 16-bit byte offsets
+  if (STORAGE != BP_STORAGE_F32 && (long long)a.rowcap * 8 >= 65536)
+    return fail(BP_ERR_UNSUPPORTED, "16-bit storage: ring rows of %d samples are too long",
+                a.rowcap);
   constexpr int threads = bp::WindowCfg<P, C::KS, C::MT, C::WS>::kThreads;
   if (batch) {
     auto kern = bp::beam_batch_kernel<P, C::KS, C::MT, C::WS, C::NSTAGE, C::SPS, C::MINB,
