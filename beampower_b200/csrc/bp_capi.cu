@@ -90,7 +90,7 @@ constexpr CfgDesc cfg_desc() {
 }
 constexpr CfgDesc kCfgDesc[kNumConfigs] = {cfg_desc<0>(), cfg_desc<1>(), cfg_desc<2>(),
                                            cfg_desc<3>(), cfg_desc<4>(), cfg_desc<5>(),
-                                           cfg_desc<6>(), cfg_desc<7>()};
+                                           cfg_desc<6>(), cfg_desc<7>(), cfg_desc<8>()};
 
 inline const CfgDesc& cfg_of(int cfg) {
   return kCfgDesc[(cfg >= 0 && cfg < kNumConfigs) ? cfg : 0];
@@ -282,6 +282,7 @@ int launch_window(int cfg, int P, bool checked, int storage, const bp::LaunchArg
     case 5: return launch_window_c<5, MAXRED>(P, checked, storage, a, batch, blocks, dev, st);
     case 6: return launch_window_c<6, MAXRED>(P, checked, storage, a, batch, blocks, dev, st);
     case 7: return launch_window_c<7, MAXRED>(P, checked, storage, a, batch, blocks, dev, st);
+    case 8: return launch_window_c<8, MAXRED>(P, checked, storage, a, batch, blocks, dev, st);
     default: return launch_window_c<0, MAXRED>(P, checked, storage, a, batch, blocks, dev, st);
   }
 }
@@ -320,6 +321,7 @@ size_t staged_smem_bytes(int cfg, int P, bool maxred, int rowcap, int max_active
     case 5: return staged_smem_cfg<5>(P, maxred, rowcap, max_active, rf);
     case 6: return staged_smem_cfg<6>(P, maxred, rowcap, max_active, rf);
     case 7: return staged_smem_cfg<7>(P, maxred, rowcap, max_active, rf);
+    case 8: return staged_smem_cfg<8>(P, maxred, rowcap, max_active, rf);
     default: return staged_smem_cfg<0>(P, maxred, rowcap, max_active, rf);
   }
 }

@@ -51,6 +51,7 @@ constexpr long long kMaxInt = std::numeric_limits<int>::max();
 //   2: 16 x 4, MT 16, SPS 2, 1/SM    3: 8 x 8, MT 8,  SPS 2, 2/SM
 //   4: 16 x 2, MT 32, SPS 1, 1/SM    5: 16 x 2, MT 32, SPS 2, 1/SM
 //   6: 8 x 8, MT 16, SPS 2, 1/SM     7: 8 x 8, MT 16, SPS 1, 1/SM
+//   8: 16 x 2, MT 16, SPS 2, 1/SM (32 sources per block)
 // Registers: a sub-partition holds 16K; 17 warps (16 consumers + producer)
 // or 2 x 9 warps put 5 warps on one sub-partition and cap a thread at 96
 // registers, 9 warps at one block per SM allow 168 (configs 6 and 7: 8 x 16
@@ -75,7 +76,8 @@ template <> struct KCfg<4> : KShape<16, 2, 32, 1, 1> {};
 template <> struct KCfg<5> : KShape<16, 2, 32, 2, 1> {};
 template <> struct KCfg<6> : KShape<8, 8, 16, 2, 1> {};
 template <> struct KCfg<7> : KShape<8, 8, 16, 1, 1> {};
-constexpr int kNumConfigs = 8;
+template <> struct KCfg<8> : KShape<16, 2, 16, 2, 1> {};
+constexpr int kNumConfigs = 9;
 constexpr int kTileSources = bp::kTableTile;
 
 // Launches the staged kernel of config CFG (plain grid of `blocks` blocks, or
@@ -98,6 +100,7 @@ BP_EXTERN_CFG(4)
 BP_EXTERN_CFG(5)
 BP_EXTERN_CFG(6)
 BP_EXTERN_CFG(7)
+BP_EXTERN_CFG(8)
 #undef BP_EXTERN_CFG
 
 }  // namespace bp_host

@@ -441,6 +441,9 @@ struct Staged {
   // whole lane up to 16; longer lanes in groups of 16, to bound registers).
   static constexpr int GS = MT > 16 ? 16 : MT;
   static_assert(MT % GS == 0, "whole groups");
+  // 16-bit storage with at most 32 accumulators per thread: the words of both
+  // sources of a metadata pair are loaded before either's arithmetic.
+  static constexpr bool PAIRLOAD = !F32 && KS * MT <= 32 && MT == GS;
 
   struct Smem {
     unsigned char* ring;
@@ -744,64 +747,57 @@ struct Staged {
         // slots are ascending sources and a strict `>` keeps the lowest
         // index among equal maxima; seeding with -FLT_MAX makes NaN and
         // -FLT_MAX (and below) lose, as in the reference's running max.
-        float bv[MT / 2][2];
-        int bi[MT / 2][2];
+        // Samples outer, so that each pair's accumulators die after use.
+        constexpr int kRows = red_rows<WS, TT>();
+        // the key of sample (q, h) into this warp's row of the max buffer, or
+        // into the single shared row (zero on entry) by an atomic max
+        auto put = [&](int q, int h, float bv, int bi) {
+          const int i = pair_sample<STORAGE>(lane, q, h);
+          const unsigned long long key = bi >= 0 ? make_key(bv, bi) : 0ull;
+          if constexpr (kRows == WS) sm.red[warp * TT + i] = key;
+          else if (key) atomicMax(&sm.red[i], key);
+        };
+        bool all_kept = true;  // warp-uniform: every slot keeps the whole tile
 #pragma unroll
-        for (int q = 0; q < MT / 2; ++q)
+        for (int k = 0; k < KS; ++k)
+          all_kept = all_kept && my_src[k].y <= t0 && t0 + TT <= my_src[k].z;
+        if (all_kept) {
 #pragma unroll
-          for (int h = 0; h < 2; ++h) {
-            bv[q][h] = -FLT_MAX;
-            bi[q][h] = -1;
-          }
+          for (int q = 0; q < MT / 2; ++q)
 #pragma unroll
-        for (int k = 0; k < KS; ++k) {
-          const int4 si = my_src[k];
-          if (si.y <= t0 && t0 + TT <= si.z) {  // warp-uniform: the whole tile is kept
+            for (int h = 0; h < 2; ++h) {
+              float bv = -FLT_MAX;
+              int bi = -1;
 #pragma unroll
-            for (int q = 0; q < MT / 2; ++q)
-#pragma unroll
-              for (int h = 0; h < 2; ++h) {
+              for (int k = 0; k < KS; ++k) {
                 const float v = h ? acc[k][q].y : acc[k][q].x;
-                if (v > bv[q][h]) {
-                  bv[q][h] = v;
-                  bi[q][h] = si.x;
+                if (v > bv) {
+                  bv = v;
+                  bi = my_src[k].x;
                 }
               }
-          } else {
+              put(q, h, bv, bi);
+            }
+        } else {
 #pragma unroll
-            for (int q = 0; q < MT / 2; ++q)
+          for (int q = 0; q < MT / 2; ++q)
 #pragma unroll
-              for (int h = 0; h < 2; ++h) {
-                const int t = t0 + pair_sample<STORAGE>(lane, q, h);
+            for (int h = 0; h < 2; ++h) {
+              const int t = t0 + pair_sample<STORAGE>(lane, q, h);
+              float bv = -FLT_MAX;
+              int bi = -1;
+#pragma unroll
+              for (int k = 0; k < KS; ++k) {
+                const int4 si = my_src[k];
                 if (t < si.y || t >= si.z) continue;  // outside the kept samples (or no source)
                 const float v = h ? acc[k][q].y : acc[k][q].x;
-                if (v > bv[q][h]) {
-                  bv[q][h] = v;
-                  bi[q][h] = si.x;
+                if (v > bv) {
+                  bv = v;
+                  bi = si.x;
                 }
               }
-          }
-        }
-        unsigned long long best[MT / 2][2];
-#pragma unroll
-        for (int q = 0; q < MT / 2; ++q)
-#pragma unroll
-          for (int h = 0; h < 2; ++h)
-            best[q][h] = bi[q][h] >= 0 ? make_key(bv[q][h], bi[q][h]) : 0ull;
-        constexpr int kRows = red_rows<WS, TT>();
-        if constexpr (kRows == WS) {
-#pragma unroll
-          for (int q = 0; q < MT / 2; ++q)
-#pragma unroll
-            for (int h = 0; h < 2; ++h)
-              sm.red[warp * TT + pair_sample<STORAGE>(lane, q, h)] = best[q][h];
-        } else {
-          // one shared row (zero on entry): max of the warps' keys
-#pragma unroll
-          for (int q = 0; q < MT / 2; ++q)
-#pragma unroll
-            for (int h = 0; h < 2; ++h)
-              if (best[q][h]) atomicMax(&sm.red[pair_sample<STORAGE>(lane, q, h)], best[q][h]);
+              put(q, h, bv, bi);
+            }
         }
         named_barrier_sync(1, NCONS);
         for (int i = tid; i < TT; i += NCONS) {
@@ -836,6 +832,90 @@ struct Staged {
     }
   }
 
+  // 16-bit storage: a weight word that skips its (source, station).
+  template <bool FAST16>
+  __device__ static __forceinline__ bool skip16(const M& m) {
+    return FAST16 ? (m.x == 0u) : (__uint_as_float(m.x) == 0.0f);
+  }
+
+  // 16-bit storage: the words of sample group g0 (runs g0 .. g0 + GS/4 - 1 of
+  // 4 samples) of every phase for one (source, station).  Each run is one
+  // 64-bit load from the copy that starts it on an 8-byte boundary (byte
+  // offsets prepared in the prologue).
+  __device__ static __forceinline__ void load16(const Smem& sm, const M& m, int sbase,
+                                                int row_words, int lane, int g0, int j,
+                                                int rowcap, int* status,
+                                                uint32_t (&wd)[P][GS / 2]) {
+    (void)j;
+    (void)rowcap;
+    (void)status;
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+      const uint2* src = reinterpret_cast<const uint2*>(
+                             sm.ring + (size_t)(sbase + p * row_words) * 4 + meta_off<P>(m, p)) +
+                         lane;
+#pragma unroll
+      for (int rr = 0; rr < GS / 4; ++rr) {
+        const int r = g0 + rr;
+#if BP_DEBUG_CHECKS
+        {  // the 4 samples of this load inside its copy's window
+          const int copy_words = rowcap >> 1;
+          const int wi = meta_off<P>(m, p) / 4 + 2 * lane + 64 * r;
+          const int cv = wi / copy_words, pos = 2 * (wi - cv * copy_words);
+          if (cv >= NVER || pos + 3 >= min(sm.st_w[j * P + p], rowcap)) {
+            atomicOr(status, kStatusBadIndex);
+            wd[p][2 * rr] = wd[p][2 * rr + 1] = 0u;
+            continue;
+          }
+        }
+#endif
+        const uint2 v = src[32 * r];  // samples 4 lane + 128 r + 0..3
+        wd[p][2 * rr] = v.x;
+        wd[p][2 * rr + 1] = v.y;
+      }
+    }
+  }
+
+  // 16-bit storage: acc += c * (phase sum) for the pairs of sample group g0.
+  template <bool FAST16>
+  __device__ static __forceinline__ void arith16(const M& m, float scale, int g0,
+                                                 const uint32_t (&wd)[P][GS / 2],
+                                                 float2 (&acc)[MT / 2]) {
+    const float c = FAST16 ? 0.0f : __uint_as_float(m.x) * scale;
+    const float2 c2 = make_float2(c, c);
+    (void)c2;
+#pragma unroll
+    for (int qq = 0; qq < GS / 2; ++qq) {
+      const int q = 2 * g0 + qq;
+      if constexpr (STORAGE == BP_STORAGE_F16) {
+        // phases summed in FP16 pairs (one extra FP16 rounding of a sum of
+        // values in [-P, P])
+        uint32_t hs = wd[0][qq];
+#pragma unroll
+        for (int p = 1; p < P; ++p) hs = hadd2_rn(hs, wd[p][qq]);
+        if constexpr (FAST16) {
+          fma2_f32_f16(acc[q], hs, m.x);
+        } else {
+          __half2 hh;
+          memcpy(&hh, &hs, 4);
+          acc[q] = __ffma2_rn(c2, __half22float2(hh), acc[q]);
+        }
+      } else {
+        // BF16: one FMA per phase and sample, phases ascending
+#pragma unroll
+        for (int p = 0; p < P; ++p) {
+          if constexpr (FAST16) {
+            fma2_f32_bf16(acc[q], wd[p][qq], m.x);
+          } else {
+            const float2 u = make_float2(__uint_as_float(wd[p][qq] << 16),
+                                         __uint_as_float(wd[p][qq] & 0xFFFF0000u));
+            acc[q] = __ffma2_rn(c2, u, acc[q]);
+          }
+        }
+      }
+    }
+  }
+
   // One active station j of the current stage for this warp's KS sources:
   // acc[k][.] += w_k * (sum over phases of the station's shifted samples).
   // FAST16 (16-bit storage, block-uniform): the weight words hold the packed
@@ -864,6 +944,16 @@ struct Staged {
         mm2[0] = mrow[k2];
         mm2[1] = mrow[k2 + 1];
       }
+      if constexpr (!F32 && PAIRLOAD) {
+        // both sources' words first, then both sources' arithmetic: two
+        // independent load batches in flight per warp
+        uint32_t wd0[P][GS / 2], wd1[P][GS / 2];
+        const bool u0 = !skip16<FAST16>(mm2[0]), u1 = !skip16<FAST16>(mm2[1]);
+        if (u0) load16(sm, mm2[0], sbase, row_words, lane, 0, j, rowcap, status, wd0);
+        if (u1) load16(sm, mm2[1], sbase, row_words, lane, 0, j, rowcap, status, wd1);
+        if (u0) arith16<FAST16>(mm2[0], scale, 0, wd0, acc[k2]);
+        if (u1) arith16<FAST16>(mm2[1], scale, 0, wd1, acc[k2 + 1]);
+      }
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
         const int k = k2 + h;
@@ -874,69 +964,13 @@ struct Staged {
           // is 2^k).  Both give the same value per sample: c times the phase
           // sum (FP16: summed in half2 first; BF16: one product per phase)
           // added to the FP32 accumulator with one rounding per product.
-          if (FAST16 ? (m.x == 0u) : (__uint_as_float(m.x) == 0.0f)) continue;  // warp-uniform
-          const float c = FAST16 ? 0.0f : __uint_as_float(m.x) * scale;
-          const float2 c2 = make_float2(c, c);
-          const uint2* src[P];  // byte offsets prepared in the prologue (multiples of 8)
-#pragma unroll
-          for (int p = 0; p < P; ++p)
-            src[p] = reinterpret_cast<const uint2*>(
-                         sm.ring + (size_t)(sbase + p * row_words) * 4 + meta_off<P>(m, p)) +
-                     lane;
+          if constexpr (PAIRLOAD) continue;  // done above for the pair
+          if (skip16<FAST16>(m)) continue;  // warp-uniform
 #pragma unroll
           for (int g0 = 0; g0 < MT / 4; g0 += GS / 4) {
             uint32_t wd[P][GS / 2];  // the group's words first
-#pragma unroll
-            for (int p = 0; p < P; ++p)
-#pragma unroll
-              for (int rr = 0; rr < GS / 4; ++rr) {
-                const int r = g0 + rr;
-#if BP_DEBUG_CHECKS
-                {  // the 4 samples of this load inside its copy's window
-                  const int copy_words = rowcap >> 1;
-                  const int wi = meta_off<P>(m, p) / 4 + 2 * lane + 64 * r;
-                  const int cv = wi / copy_words, pos = 2 * (wi - cv * copy_words);
-                  if (cv >= NVER || pos + 3 >= min(sm.st_w[j * P + p], rowcap)) {
-                    atomicOr(status, kStatusBadIndex);
-                    wd[p][2 * rr] = wd[p][2 * rr + 1] = 0u;
-                    continue;
-                  }
-                }
-#endif
-                const uint2 v = src[p][32 * r];  // samples 4 lane + 128 r + 0..3
-                wd[p][2 * rr] = v.x;
-                wd[p][2 * rr + 1] = v.y;
-              }
-#pragma unroll
-            for (int qq = 0; qq < GS / 2; ++qq) {
-              const int q = 2 * g0 + qq;
-              if constexpr (STORAGE == BP_STORAGE_F16) {
-                // phases summed in FP16 pairs (one extra FP16 rounding of a
-                // sum of values in [-P, P])
-                uint32_t hs = wd[0][qq];
-#pragma unroll
-                for (int p = 1; p < P; ++p) hs = hadd2_rn(hs, wd[p][qq]);
-                if constexpr (FAST16) {
-                  fma2_f32_f16(acc[k][q], hs, m.x);
-                } else {
-                  __half2 hh;
-                  memcpy(&hh, &hs, 4);
-                  acc[k][q] = __ffma2_rn(c2, __half22float2(hh), acc[k][q]);
-                }
-              } else {
-                // BF16: one FMA per phase and sample, phases ascending
-#pragma unroll
-                for (int p = 0; p < P; ++p) {
-                  if constexpr (FAST16) {
-                    fma2_f32_bf16(acc[k][q], wd[p][qq], m.x);
-                  } else {
-                    const float2 u = make_float2(__uint_as_float(wd[p][qq] << 16),
-                                                 __uint_as_float(wd[p][qq] & 0xFFFF0000u));
-                    acc[k][q] = __ffma2_rn(c2, u, acc[k][q]);
-                  }
-                }
-              }
-            }
+            load16(sm, m, sbase, row_words, lane, g0, j, rowcap, status, wd);
+            arith16<FAST16>(m, scale, g0, wd, acc[k]);
           }
         } else if constexpr (CHECKED) {
           const float w = __uint_as_float(m.x);
