@@ -111,10 +111,12 @@ int pick_config(int storage, bool maxred) {
     const int c = g_cfg_choice[storage][maxred ? 1 : 0].load();
     if (c >= 0 && c < kNumConfigs) return c;
   }
-  // Built-in defaults, measured on B200 (400,000 sources x 60 stations):
-  // FP32 storage is shared-memory bound and favours config 0; 16-bit storage
-  // is issue bound and gains from config 1's longer time tiles.
-  return storage == BP_STORAGE_F32 ? 0 : 1;
+  // Built-in defaults, measured on B200 (400,000 sources x 60 stations x
+  // 180,000 samples, reduce='max'): FP32 storage runs fastest with config 8
+  // (32-source blocks, 721 ms; config 3 741 ms, config 0 757 ms), 16-bit
+  // storage with config 2 (16 warps x 4 sources x 16 samples, two stations
+  // per ring stage; FP16 471 ms, BF16 510 ms).
+  return storage == BP_STORAGE_F32 ? 8 : 2;
 }
 
 }  // namespace

@@ -50,7 +50,7 @@ def test_batch_matches_single_windows(cuda, oracle_lib):
     rng, A, grids = _network(1)
     tables = [TravelTimeTable(D, W) for D, W in grids]
     windows = _windows(rng, A.shape[0])
-    batch = WindowBatch(tables, windows, A)
+    batch = WindowBatch(tables, windows, A, storage="fp32")
     feats = []
     for i, w in enumerate(windows):
         F = np.abs(rng.standard_normal((A.shape[0], A.shape[1], w.n_samples))).astype(np.float32)
@@ -76,7 +76,7 @@ def test_batch_graph_replay_new_data(cuda, oracle_lib):
     rng, A, grids = _network(2)
     tables = [TravelTimeTable(D, W) for D, W in grids]
     windows = _windows(rng, A.shape[0])
-    batch = WindowBatch(tables, windows, A)
+    batch = WindowBatch(tables, windows, A, storage="fp32")
     batch.capture()
     for _ in range(2):
         feats = []

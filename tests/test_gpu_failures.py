@@ -62,7 +62,7 @@ def test_scheduler_respects_memory_budget(cuda):
     A = rng.uniform(0.2, 1.2, size=(S, C, P)).astype(np.float32)
     D = rng.integers(0, 100, size=(N, S, P)).astype(np.int32)
     W = np.ones((N, S), np.float32)
-    ns = NetworkStream(TravelTimeTable(D, W), A)
+    ns = NetworkStream(TravelTimeTable(D, W), A, storage="fp32")
     budget = int(1.5 * ns.bytes_per_chunk(500))
     sched = StreamScheduler({"n": ns}, max_inflight=8, memory_budget=budget)
     peak = 0
@@ -86,7 +86,7 @@ def _two_networks(rng):
         A = rng.uniform(0.2, 1.2, size=(S, C, P)).astype(np.float32)
         D = rng.integers(0, 80, size=(N, S, P)).astype(np.int32)
         W = np.ones((N, S), np.float32)
-        nets[name] = NetworkStream(TravelTimeTable(D, W), A)
+        nets[name] = NetworkStream(TravelTimeTable(D, W), A, storage="fp32")
         data[name] = (A, D, W, np.abs(rng.standard_normal((S, C, 1500))).astype(np.float32))
     return nets, data
 

@@ -1,11 +1,16 @@
 """16-bit trace storage (BF16 / FP16 with a power-of-two per-station scale,
 FP32 accumulation) against the float64 restatement of the reference.
 
-Tolerances, relative to |beam| in float64 (all terms of these cases have
-one sign, so the beam's relative error is bounded by one rounding of the
-stored values):
-  FP16 storage: 1e-3 (11 significant bits: unit roundoff 2^-11 = 4.9e-4)
-  BF16 storage: 4e-3 (8 significant bits: unit roundoff 2^-8 = 3.9e-3)
+Tolerances, relative to |beam| in float64.  All terms of these cases have
+one sign, so the beam's relative error is bounded by the relative roundings
+each term goes through, plus FP32 accumulation (n 2^-24, below 1e-5 here):
+  FP16 storage: 1e-3.  11 significant bits, unit roundoff 2^-11 = 4.9e-4;
+    a term is rounded once when stored and once more in the FP16 sum of its
+    phases: at most 2 x 4.9e-4 = 9.8e-4.
+  BF16 storage: 2e-3.  8 significant bits, unit roundoff 2^-9 = 1.95e-3;
+    a term is rounded once, when stored (each phase has its own FP32 FMA).
+    BF16 therefore cannot promise 1e-3: a single stored value may be off by
+    1.95e-3, and beams of few terms can keep most of that.
 Argmax: identical wherever the float64 top-two margin exceeds the tolerance.
 """
 import numpy as np
@@ -15,7 +20,7 @@ from conftest import load_golden
 
 pytestmark = pytest.mark.gpu
 
-TOL = {"fp16": 1e-3, "bf16": 4e-3}
+TOL = {"fp16": 1e-3, "bf16": 2e-3}
 
 
 def _margin_mask(beam64, valid, tol):
@@ -160,3 +165,48 @@ def test_16bit_nan_in_weighted_trace(cuda, orc, storage):
     with np.errstate(invalid="ignore"):  # -inf - -inf at samples with no candidate
         sure = has & ((top1 - top2) > tol * np.abs(top1))
     assert np.array_equal(am[sure], order[0][sure])
+
+
+@pytest.mark.parametrize("spec_name", ["small-4k-src-20-sta-6000-samples", "small-heavy-tailed"])
+def test_scheduler_default_storage_within_1e3(cuda, orc, spec_name):
+    """The batch and stream schedulers at their default storage (FP16):
+    beam_max within 1e-3 of float64 and argmax identical above the margin,
+    on the Gaussian and the heavy-tailed network (first 1,000 sources)."""
+    import inspect
+    import torch
+    from beampower_b200.batch import Window, WindowBatch
+    from beampower_b200.stream import NetworkStream
+    from beampower_b200.synthetic import SPECS, make_workload
+    from beampower_b200.tables import TravelTimeTable
+    defaults = {inspect.signature(WindowBatch).parameters["storage"].default,
+                inspect.signature(NetworkStream).parameters["storage"].default}
+    assert defaults == {"fp16"}
+    tol = 1e-3
+    wl = make_workload(SPECS[spec_name])
+    n = 1000
+    F, A = wl["waveform_features"], wl["weights_phases"]
+    D, W = wl["time_delays"][:n], wl["weights_sources"][:n]
+    T = F.shape[2]
+    beam64, valid = orc.fp64_beams(orc.fp64_prestack(F, A), D, W, 0)
+    sure, arg64, top1 = _margin_mask(beam64, valid, tol)
+    has = np.isfinite(top1)
+
+    def check(bm, am, who):
+        rel = np.abs(bm[has] - top1[has]) / np.abs(top1[has])
+        assert rel.max() <= tol, (who, rel.max())
+        assert np.array_equal(am[sure], arg64[sure]), who
+
+    table = TravelTimeTable(D, W)
+    batch = WindowBatch([table], [Window(0, T)], A)
+    batch.set_features(0, F)
+    (bm, am), = batch.run()
+    torch.cuda.synchronize()
+    check(bm.cpu().numpy(), am.cpu().numpy(), "batch")
+    batch.close()
+    ns = NetworkStream(table, A)
+    for a in range(0, T, 1700):
+        ns.push(F[:, :, a:a + 1700])
+    ns.flush()
+    bm, am = ns.collect()
+    check(bm, am, "stream")
+    table.close()

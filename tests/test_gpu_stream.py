@@ -62,14 +62,17 @@ def test_stream_16bit_within_tolerance(cuda, orc):
     assert rel.max() <= 1e-3
 
 
-def test_scheduler_mix_equals_alone(cuda):
+@pytest.mark.parametrize("storage", ["fp32", "fp16"])
+def test_scheduler_mix_equals_alone(cuda, storage):
     """Two networks' chunks interleaved through the continuous-batching
-    scheduler (3 slots): each network's output equals its output alone."""
+    scheduler (3 slots): each network's output equals its output alone (bit
+    for bit: a chunk's arithmetic does not depend on what runs beside it)."""
     from beampower_b200.stream import NetworkStream, StreamScheduler
     from beampower_b200.tables import TravelTimeTable
     nets = {"a": _net(21, N=900, S=8), "b": _net(22, N=300, S=5, dhi=120)}
-    alone = {k: _stream(*v, "strict") for k, v in nets.items()}
-    streams = {k: NetworkStream(TravelTimeTable(v[1], v[2]), v[0], "strict", name=k)
+    alone = {k: _stream(*v, "strict", storage=storage) for k, v in nets.items()}
+    streams = {k: NetworkStream(TravelTimeTable(v[1], v[2]), v[0], "strict", storage=storage,
+                                 name=k)
                for k, v in nets.items()}
     sched = StreamScheduler(streams, max_inflight=3, memory_budget=2e9)
     offs = {k: 0 for k in nets}
@@ -99,7 +102,7 @@ def test_checkpoint_and_resume_equals_offline(cuda, oracle_lib, tmp_path, oob, d
     from beampower_b200.stream import NetworkStream
     from beampower_b200.tables import TravelTimeTable
     A, D, W, F = _net(30 + cut + abs(dlo), dlo=dlo)
-    first = NetworkStream(TravelTimeTable(D, W), A, out_of_bounds=oob)
+    first = NetworkStream(TravelTimeTable(D, W), A, out_of_bounds=oob, storage="fp32")
     t = 0
     for L in CHUNKS[:cut]:
         first.push(F[:, :, t:t + L])
@@ -107,7 +110,8 @@ def test_checkpoint_and_resume_equals_offline(cuda, oracle_lib, tmp_path, oob, d
     bm1, am1 = first.collect()
     path = tmp_path / "stream_state.npz"
     first.save(path)
-    second = NetworkStream(TravelTimeTable(D, W), A, out_of_bounds=oob).load(path)
+    second = NetworkStream(TravelTimeTable(D, W), A, out_of_bounds=oob,
+                           storage="fp32").load(path)
     for L in CHUNKS[cut:]:
         second.push(F[:, :, t:t + L])
         t += L
@@ -123,9 +127,9 @@ def test_restore_rejects_another_network(cuda):
     from beampower_b200.stream import NetworkStream
     from beampower_b200.tables import TravelTimeTable
     A, D, W, F = _net(41)
-    a = NetworkStream(TravelTimeTable(D, W), A)
+    a = NetworkStream(TravelTimeTable(D, W), A, storage="fp32")
     a.push(F[:, :, :700])
     st = a.state()
     A2, D2, W2, _ = _net(42, N=500)
     with pytest.raises(ValueError):
-        NetworkStream(TravelTimeTable(D2, W2), A2).restore(st)
+        NetworkStream(TravelTimeTable(D2, W2), A2, storage="fp32").restore(st)
