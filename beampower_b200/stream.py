@@ -15,17 +15,22 @@ carried halo and the stream position, so a stream can resume in another
 process and still give the offline results.
 
 ``StreamScheduler`` is the request loop over many networks (continuous
-batching): chunks are queued on arrival and admitted while fewer than
-``max_inflight`` chunks are on the GPU and their memory fits the budget; each
-network's chunks run in order on its own CUDA stream, chunks of different
-networks overlap on the device.  Latency is arrival (host clock) to the
-completion event of the chunk's last kernel (device clock, mapped to the host
-clock once).
+batching): chunks are queued on arrival and admitted, earliest deadline first
+(arrival + the latency budget), while fewer than ``max_inflight`` chunks are
+on the GPU and their memory fits the budget.  Chunks of different networks
+overlap on the device; a network's chunks run in order (each waits for the
+previous one's completion event).  With ``priorities`` the admitted chunks
+run on CUDA streams of graded priority: a chunk admitted while k older chunks
+are in flight gets the k-th highest priority, so the SMs serve the oldest
+deadline first instead of sharing them evenly among all chunks in flight.
+Latency is arrival (host clock) to the completion event of the chunk's last
+kernel (device clock, mapped to the host clock once).
 """
+import heapq
 from __future__ import annotations
 
-import collections
 import ctypes as ct
+import itertools
 import time
 
 import numpy as np
@@ -74,6 +79,9 @@ class NetworkStream:
         self.carry = torch.zeros((self.S, self.C, -self.lead), dtype=torch.float32,
                                  device=self.device)  # global [t_emit + lead, t_end)
         self.stream = torch.cuda.Stream(device=self.device)
+        # completion event of the last chunk's work (first: the carry's fill)
+        self.done = torch.cuda.Event()
+        self.done.record(torch.cuda.current_stream(self.device))
         self.results = []  # (g0, beam_max, argmax) device tensors, in order
 
     def bytes_per_chunk(self, n_samples):
@@ -122,11 +130,28 @@ class NetworkStream:
             t.record_stream(torch.cuda.current_stream())
         return bm, am
 
-    def push(self, chunk):
+    def _enter(self, stream):
+        """Make `stream` (default: this network's own) wait for the previous
+        chunk's work; returns it."""
+        s = self.stream if stream is None else stream
+        s.wait_event(self.done)
+        # the carried halo was written on the previous chunk's stream
+        self.carry.record_stream(s)
+        return s
+
+    def _leave(self, s):
+        self.done = torch.cuda.Event()
+        self.done.record(s)
+
+    def push(self, chunk, stream=None, start_event=None):
         """Append an (S, C, L) chunk (numpy, host or device tensor); enqueue the
-        work on this network's stream.  Returns the emitted (g0, beam_max,
-        argmax) or None."""
-        with torch.cuda.stream(self.stream):
+        work on `stream` (default: this network's own stream), after the
+        previous chunk's work; `start_event` is recorded where the chunk's
+        own work starts.  Returns the emitted (g0, beam_max, argmax) or None."""
+        s = self._enter(stream)
+        if start_event is not None:
+            start_event.record(s)
+        with torch.cuda.stream(s):
             if isinstance(chunk, np.ndarray):
                 chunk = torch.from_numpy(np.ascontiguousarray(chunk, dtype=np.float32))
             chunk = chunk.to(self.device, dtype=torch.float32, non_blocking=True)
@@ -143,11 +168,13 @@ class NetworkStream:
                 self.t_emit = emit_to
             new_base = self.t_emit + self.lead
             self.carry = record[:, :, new_base - base:].contiguous()
+        self._leave(s)
         return out
 
-    def flush(self):
+    def flush(self, stream=None):
         """End of the record: emit every remaining sample."""
-        with torch.cuda.stream(self.stream):
+        s = self._enter(stream)
+        with torch.cuda.stream(s):
             base = self.t_emit + self.lead
             out = None
             if self.t_end > self.t_emit:
@@ -156,7 +183,13 @@ class NetworkStream:
                 out = (self.t_emit, bm, am)
                 self.results.append(out)
                 self.t_emit = self.t_end
+        self._leave(s)
         return out
+
+    def synchronize(self):
+        """Wait for every chunk enqueued so far."""
+        self.stream.synchronize()
+        self.done.synchronize()
 
     # ---- checkpoint / resume ------------------------------------------------
     def state(self):
@@ -164,7 +197,7 @@ class NetworkStream:
         not-yet-emitted features (the max-delay halo) and the stream position.
         Results already emitted are the caller's (``collect``) and are not in
         the snapshot.  Synchronises the stream."""
-        self.stream.synchronize()
+        self.synchronize()
         info = self.table.info
         return {"carry": self.carry.cpu().numpy(), "t_end": self.t_end,
                 "t_emit": self.t_emit, "lead": self.lead, "lag": self.lag,
@@ -187,8 +220,10 @@ class NetworkStream:
         if carry.shape != (self.S, self.C, int(state["t_end"]) - int(state["t_emit"])
                            - self.lead):
             raise ValueError("snapshot carry does not match its stream position")
+        self.synchronize()
         with torch.cuda.stream(self.stream):
             self.carry = torch.from_numpy(np.ascontiguousarray(carry)).to(self.device)
+        self._leave(self.stream)
         self.t_end = int(state["t_end"])
         self.t_emit = int(state["t_emit"])
         self.results = []
@@ -205,7 +240,7 @@ class NetworkStream:
 
     def collect(self):
         """All emitted results as numpy arrays (synchronises the stream)."""
-        self.stream.synchronize()
+        self.synchronize()
         if not self.results:
             return np.zeros(0, np.float32), np.zeros(0, np.int32)
         bm = torch.cat([r[1] for r in self.results]).cpu().numpy()
@@ -225,25 +260,47 @@ class StreamScheduler:
         later pending chunks are dropped (``timed_out``) and the network
         takes no more chunks.  ``cancel(name)`` ends a stream the same way on
         request; chunks already on the GPU complete.
+    latency_budget: seconds from arrival to result that a chunk aims for; its
+        deadline is arrival + budget (a dict gives per-network budgets).
+        Pending chunks are admitted earliest deadline first; a network's own
+        chunks keep their order (their deadlines increase with arrival).
+    priorities: run admitted chunks on a pool of streams of graded priority
+        (the device's range, highest first), the k-th oldest chunk in flight
+        on the k-th highest; False: every chunk on its network's own stream.
     """
 
-    def __init__(self, networks, max_inflight=8, memory_budget=150e9, max_wait=None):
+    def __init__(self, networks, max_inflight=8, memory_budget=150e9, max_wait=None,
+                 latency_budget=0.05, priorities=True):
         self.networks = dict(networks)
         self.max_inflight = max_inflight
         self.memory_budget = memory_budget
         self.max_wait = max_wait
+        self.latency_budget = latency_budget
+        self._seq = itertools.count()
         self.closed = {}  # name -> "cancelled" or "timed out"
         self.peak_pending = 0  # deepest queue seen
         self.peak_inflight = 0
         self.peak_mem = 0  # most device bytes admitted at once
         self.cancelled = []  # (name, arrival) of chunks dropped by cancel()
         self.timed_out = []  # (name, arrival) of chunks dropped by max_wait
-        self.pending = collections.deque()  # (arrival, name, chunk)
-        self.inflight = []  # (arrival, name, event, bytes, terms)
+        self.pending = []  # heap of (deadline, seq, arrival, name, chunk)
+        self.inflight = []  # (arrival, name, event, bytes, terms, admit, start event)
         self.mem_in_use = 0
         self.done = []  # (name, arrival, completion, terms)
         dev = next(iter(self.networks.values())).device
         self.device = dev
+        # streams of distinct priorities, highest first (priorities outside the
+        # device's range are clamped by CUDA, so the pool stops at a repeat)
+        self.prio_streams = []
+        if priorities:
+            seen = set()
+            for k in range(16):
+                st = torch.cuda.Stream(device=dev, priority=-k)
+                if st.priority in seen:
+                    break
+                seen.add(st.priority)
+                self.prio_streams.append(st)
+            self.prio_streams.sort(key=lambda st: st.priority)
         # device clock -> host clock
         torch.cuda.synchronize(dev)
         self._ev0 = torch.cuda.Event(enable_timing=True)
@@ -256,17 +313,21 @@ class StreamScheduler:
             raise KeyError(f"unknown network {name!r}")
         if name in self.closed:
             raise ValueError(f"network {name!r} takes no more chunks ({self.closed[name]})")
-        self.pending.append((time.perf_counter() if arrival is None else arrival, name, chunk))
+        arrival = time.perf_counter() if arrival is None else arrival
+        budget = (self.latency_budget.get(name, 0.05) if isinstance(self.latency_budget, dict)
+                  else self.latency_budget)
+        heapq.heappush(self.pending, (arrival + budget, next(self._seq), arrival, name, chunk))
 
     def _drop(self, name, reason, into):
         """End network `name`'s stream: its pending chunks leave the queue."""
         self.closed[name] = reason
-        keep = collections.deque()
-        for item in self.pending:
-            if item[1] == name:
-                into.append((name, item[0]))
+        keep = []
+        for item in sorted(self.pending):
+            if item[3] == name:
+                into.append((name, item[2]))
             else:
                 keep.append(item)
+        heapq.heapify(keep)
         self.pending = keep
 
     def cancel(self, name):
@@ -278,7 +339,7 @@ class StreamScheduler:
 
     def _admit(self):
         while self.pending and len(self.inflight) < self.max_inflight:
-            arrival, name, chunk = self.pending[0]
+            _deadline, _seq, arrival, name, chunk = self.pending[0]
             if self.max_wait is not None and time.perf_counter() - arrival > self.max_wait:
                 self._drop(name, "timed out", self.timed_out)
                 continue
@@ -287,15 +348,17 @@ class StreamScheduler:
             free, _ = torch.cuda.mem_get_info(self.device)
             if self.inflight and (self.mem_in_use + need > self.memory_budget or need > free):
                 break  # wait for memory to free up
-            self.pending.popleft()
+            heapq.heappop(self.pending)
             admit = time.perf_counter()
             t_emit0 = net.t_emit
+            stream = None
+            if self.prio_streams:
+                stream = self.prio_streams[min(len(self.inflight), len(self.prio_streams) - 1)]
             ev0 = torch.cuda.Event(enable_timing=True)
-            ev0.record(net.stream)
-            net.push(chunk)
+            net.push(chunk, stream=stream, start_event=ev0)
             terms = (net.t_emit - t_emit0) * net.table.n_sources * net.S * net.P
             ev = torch.cuda.Event(enable_timing=True)
-            ev.record(net.stream)
+            ev.record(net.stream if stream is None else stream)
             self.inflight.append((arrival, name, ev, need, terms, admit, ev0))
             self.mem_in_use += need
 

@@ -133,3 +133,35 @@ def test_restore_rejects_another_network(cuda):
     A2, D2, W2, _ = _net(42, N=500)
     with pytest.raises(ValueError):
         NetworkStream(TravelTimeTable(D2, W2), A2, storage="fp32").restore(st)
+
+
+def test_scheduler_earliest_deadline_first(cuda):
+    """Admission order is earliest deadline first (arrival + the network's
+    latency budget) while each network's chunks stay in order; the priority
+    pool holds streams of distinct, increasing priority values (highest
+    first); results equal each network alone."""
+    from beampower_b200.stream import NetworkStream, StreamScheduler
+    from beampower_b200.tables import TravelTimeTable
+    nets = {"a": _net(31, N=400, S=6), "b": _net(32, N=200, S=5, dhi=120)}
+    alone = {k: _stream(*v, "strict", storage="fp16") for k, v in nets.items()}
+    streams = {k: NetworkStream(TravelTimeTable(v[1], v[2]), v[0], "strict", name=k)
+               for k, v in nets.items()}
+    sched = StreamScheduler(streams, max_inflight=1, latency_budget={"a": 1.0, "b": 0.01})
+    prios = [s.priority for s in sched.prio_streams]
+    assert prios and prios == sorted(set(prios))
+    offs = {k: 0 for k in nets}
+    t0 = 1000.0
+    for i, L in enumerate(CHUNKS):
+        for k, v in nets.items():
+            sched.submit(k, v[3][:, :, offs[k]:offs[k] + L], arrival=t0 + 0.001 * i)
+            offs[k] += L
+    sched.drain()
+    # one chunk in flight at a time: completion order is admission order;
+    # every chunk of b (deadline arrival + 10 ms) comes before a's (+ 1 s)
+    order = [x[0] for x in sched.done]
+    assert order == ["b"] * len(CHUNKS) + ["a"] * len(CHUNKS)
+    for k, ns in streams.items():
+        ns.flush()
+        bm, am = ns.collect()
+        assert np.array_equal(bits(bm), bits(alone[k][0])), k
+        assert np.array_equal(am, alone[k][1]), k
