@@ -54,7 +54,9 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--n-sources", type=int, default=None,
                     help="keep only the first n sources (profiling runs on a smaller case)")
-    ap.add_argument("--storage", default="fp32", choices=["fp32", "bf16", "fp16"])
+    ap.add_argument("--storage", default=None, choices=["fp32", "bf16", "fp16"],
+                    help="trace storage (default: fp32 for the large workload, fp16 for "
+                         "batch and serving)")
     ap.add_argument("--workload", default="large", choices=["large", "batch", "serving", "stages"],
                     help="large: the 400k-source plain call (default); batch: 128 windows "
                          "in one persistent launch vs one call per window; serving: "
@@ -72,6 +74,14 @@ def parse():
     ap.add_argument("--profile", action="store_true",
                     help="timed steps only: no end-to-end pass, no baselines")
     return ap.parse_args()
+
+
+def large_config(N, S, P, T, out_of_bounds, storage):
+    """The `config` of the large workload, the same in both arms."""
+    return {"workload": LARGE.name, "n_sources": N, "n_stations": S, "n_phases": P,
+            "n_samples": T, "reduce": "max", "out_of_bounds": out_of_bounds,
+            "storage": storage, "parallelism": "replicas",
+            "l2": "inputs 418 MB > L2, no flush"}
 
 
 def effective_terms(D, W, T, flexible):
@@ -257,6 +267,116 @@ print(json.dumps({"value": m * T * S * P / dt, "seconds": dt, "sources": m}))
         return {"unavailable": "timed out"}
 
 
+_SAMPLED_CHILD = r"""
+import sys, json, time, ctypes as ct
+import numpy as np
+sys.path.insert(0, %r)
+from oracle.oracle import Reference, REF_GPU_SO
+job = json.loads(sys.argv[1])
+ref = Reference()
+if job["kind"] == "batch":
+    from beampower_b200.synthetic import make_batch_workload, window_features
+    wl = make_batch_workload()
+    A = wl["weights_phases"]
+
+    def item(i):
+        w = wl["windows"][i]
+        D, W = wl["grids"][w["table"]]
+        m = np.zeros(W.shape[1], np.float32)
+        m[w["stations"]] = 1.0
+        return window_features(wl, i), A, D, W * m[None, :], len(w["stations"]), w["n_samples"]
+else:
+    from beampower_b200.synthetic import make_serving_networks, serving_record
+    nets = make_serving_networks()
+
+    def item(i):
+        n = nets[i]
+        D, W = n["delays"], n["weights"]
+        lag = int(D.max())
+        F, _ = serving_record(n, 2)
+        L = n["chunk"]
+        # one chunk's record: the chunk plus the max-delay halo it needs
+        return (np.ascontiguousarray(F[:, :, :L + lag]), n["weights_phases"], D, W,
+                n["n_stations"], L)
+gpu = job["mode"] == "gpu"
+if gpu:
+    lib = ct.CDLL(REF_GPU_SO)
+    f32p, i32p, sz = ct.POINTER(ct.c_float), ct.POINTER(ct.c_int), ct.c_size_t
+    lib.beamform_max.argtypes = [f32p, i32p, f32p, sz, sz, sz, sz, ct.c_int, f32p, i32p]
+    lib.beamform_max.restype = None
+
+
+def run(F, A, D, W, n_sub):
+    stride = max(1, D.shape[0] // n_sub)
+    idx = np.arange(0, D.shape[0], stride)[:n_sub]
+    d = np.ascontiguousarray(D[idx])
+    w = np.ascontiguousarray(W[idx])
+    if not gpu:
+        t0 = time.perf_counter()
+        U = ref.prestack(F, A, -1)
+        ref.beamform_max(U, d, w, 0, -1)
+        return time.perf_counter() - t0, len(idx)
+    U = np.ascontiguousarray(ref.prestack(F, A, -1))
+    S, T, P = U.shape
+    # masked stations are read by the reference CUDA kernel (beamform.cu:109-115):
+    # clamp their delays into the trace (output-neutral for the CPU semantics)
+    mask = w != 0
+    big = np.iinfo(np.int32).max
+    dmin = np.where(mask[:, :, None], d, big).min(axis=(1, 2))
+    dmin = np.where(dmin == big, 0, dmin).astype(np.int32)
+    d = np.ascontiguousarray(np.where(mask[:, :, None], d, dmin[:, None, None]).astype(np.int32))
+    bm = np.zeros(T, np.float32)
+    am = np.zeros(T, np.int32)
+    t0 = time.perf_counter()
+    lib.beamform_max(U.ctypes.data_as(f32p), d.ctypes.data_as(i32p), w.ctypes.data_as(f32p),
+                     T, len(idx), S, P, 0, bm.ctypes.data_as(f32p), am.ctypes.data_as(i32p))
+    return time.perf_counter() - t0, len(idx)
+
+
+items = job["items"]
+per_item = job["target_s"] / max(1, len(items))
+terms = secs = 0.0
+done = []
+for i in items:
+    F, A, D, W, s_used, t_out = item(i)
+    P = D.shape[2]
+    dt, m = run(F, A, D, W, 128)
+    n_sub = int(min(D.shape[0], max(128, 128 * per_item / max(dt, 1e-4))))
+    dt, m = run(F, A, D, W, n_sub)
+    terms += float(m) * t_out * s_used * P
+    secs += dt
+    done.append([int(i), int(m), int(D.shape[0])])
+print(json.dumps({"terms": terms, "seconds": secs, "items": done}))
+"""
+
+
+def sampled_reference(kind, mode, items, target_s, timeout=900):
+    """The reference's own CPU library (mode 'cpu', all host threads) or its
+    CUDA path (mode 'gpu', oracle/_ref/beamform_gpu.so on one GPU, host
+    buffers, H2D included) on a sample of batch windows or serving chunks,
+    in a child process: each item with an evenly strided source subsample
+    sized for about target_s / len(items) seconds.  Returns the nominal beam
+    terms per second of the sample (window or chunk terms, the sources the
+    sample kept)."""
+    from oracle.oracle import REF_CPU_SO, REF_GPU_SO
+    so = REF_GPU_SO if mode == "gpu" else REF_CPU_SO
+    if not os.path.exists(so):
+        return {"unavailable": f"{os.path.relpath(so, ROOT)} not built"}
+    job = json.dumps({"kind": kind, "mode": mode, "items": list(items), "target_s": target_s})
+    try:
+        out = subprocess.run([sys.executable, "-c", _SAMPLED_CHILD % ROOT, job],
+                             capture_output=True, text=True, timeout=timeout)
+    except subprocess.TimeoutExpired:
+        return {"unavailable": "timed out"}
+    line = [ln for ln in out.stdout.splitlines() if ln.startswith("{")]
+    if out.returncode != 0 or not line:
+        return {"unavailable": f"exit {out.returncode}: {out.stderr.strip()[-200:]}"}
+    r = json.loads(line[-1])
+    return {"value": r["terms"] / r["seconds"], "unit": "beam terms/s",
+            "sample_terms": r["terms"], "sample_seconds": r["seconds"],
+            "items": r["items"]}
+
+
 # ----------------------------------------------------------------------------
 
 def run_reference_arm(args, rank, world):
@@ -286,15 +406,15 @@ def run_reference_arm(args, rank, world):
     line = {
         "impl": "reference", "metric": "beam terms/s (src x t x sta x phase)",
         "value": value, "unit": "beam terms/s", "n_gpus": args.gpus, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms_full, "higher_is_better": True,
+        "warmup": args.warmup, "ms_per_step": statistics.mean(times) * 1e3,
+        "ms_per_step_full_workload": ms_full, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": LARGE.name, "n_sources": N, "n_stations": S, "n_phases": P,
-                   "n_samples": T, "reduce": "max", "out_of_bounds": args.out_of_bounds,
-                   "storage": "fp32", "parallelism": "replicas"},
+        "config": large_config(N, S, P, T, args.out_of_bounds, "fp32"),
         "cpu_baseline": {"value": value, "unit": "beam terms/s", "cores": threads, "kind": kind,
                          "sample": f"{n_sub} of {N} sources (every k-th), all {T} samples, "
-                                   "prestack + beamform_max per step; ms_per_step "
-                                   "extrapolated to the full workload"},
+                                   "prestack + beamform_max per step (ms_per_step: one "
+                                   "sampled step; ms_per_step_full_workload: the whole "
+                                   "workload at the same rate)"},
         "e2e": {"value": value, "unit": "beam terms/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -456,22 +576,26 @@ def run_ours(args, rank, world, local_rank):
             tdist.destroy_process_group()
         return
 
-    # ---- end to end through the public numpy API, pinned host inputs ----
-    pin = {k: torch.from_numpy(v).pin_memory() for k, v in
-           (("F", F), ("A", A), ("D", D), ("W", W))}
-    hF, hA, hD, hW = (pin[k].numpy() for k in ("F", "A", "D", "W"))
-    bp.beamform(hF, hD, hA, hW, reduce="max", out_of_bounds=args.out_of_bounds,
-                storage=args.storage)
-    e2e_times = []
-    for _ in range(max(2, min(args.steps, 3))):
-        barrier(dev)
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
+    # ---- end to end through the public numpy API: host inputs copied in and
+    # results copied out inside the timed region, on pageable arrays (what
+    # the reference's callers pass, beampower.py:108-110) and on pinned ones
+    def e2e(hF, hD, hA, hW):
         bp.beamform(hF, hD, hA, hW, reduce="max", out_of_bounds=args.out_of_bounds,
                     storage=args.storage)
-        e2e_times.append(time.perf_counter() - t0)
-    e2e_s = statistics.mean(e2e_times)
-    e2e_s = max_over_ranks(e2e_s, dev)
+        times = []
+        for _ in range(max(2, min(args.steps, 3))):
+            barrier(dev)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            bp.beamform(hF, hD, hA, hW, reduce="max", out_of_bounds=args.out_of_bounds,
+                        storage=args.storage)
+            times.append(time.perf_counter() - t0)
+        return max_over_ranks(statistics.mean(times), dev)
+
+    e2e_s = e2e(F, D, A, W)
+    pin = {k: torch.from_numpy(v).pin_memory() for k, v in
+           (("F", F), ("A", A), ("D", D), ("W", W))}
+    e2e_pinned_s = e2e(*(pin[k].numpy() for k in ("F", "D", "A", "W")))
     h2d = F.nbytes + A.nbytes + D.nbytes + W.nbytes
     d2h = 8 * T
 
@@ -503,10 +627,7 @@ def run_ours(args, rank, world, local_rank):
             "vs_baseline": None,
             "dtype": "f32",
             "data": "synthetic",
-            "config": {"workload": LARGE.name, "n_sources": N, "n_stations": S, "n_phases": P,
-                       "n_samples": T, "reduce": "max", "out_of_bounds": args.out_of_bounds,
-                       "storage": args.storage, "parallelism": f"replicas{world}",
-                       "l2": "inputs 418 MB > L2, no flush"},
+            "config": large_config(N, S, P, T, args.out_of_bounds, args.storage),
             "effective_terms_per_step": eff,
             "nominal_terms_per_step": terms,
             "breakdown_ms": {"table_build": table_ms, "prestack": prestack_ms,
@@ -530,7 +651,9 @@ def run_ours(args, rank, world, local_rank):
             "run_variants": run_variants,
             "e2e": {"value": world * terms / e2e_s, "unit": "beam terms/s",
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                    "seconds_per_step": e2e_s},
+                    "seconds_per_step": e2e_s, "host_inputs": "pageable numpy arrays",
+                    "pinned": {"value": world * terms / e2e_pinned_s,
+                               "seconds_per_step": e2e_pinned_s}},
             "gpu_launches": int(launches),
             "clocks": clocks,
         }
@@ -564,6 +687,8 @@ class ctypes_double:
 
 def main():
     args = parse()
+    if args.storage is None:
+        args.storage = "fp16" if args.workload in ("batch", "serving") else "fp32"
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local_rank = int(os.environ.get("LOCAL_RANK", 0))
@@ -593,7 +718,10 @@ def main():
 def run_batch(args, local_rank):
     """128 detection windows (3,000-90,000 samples, 20-80 of 100 stations, a
     400,000- or 50,000-source grid each): one persistent launch replayed from
-    a CUDA graph, against the plain path called once per window."""
+    a CUDA graph, against (1) this library's plain path called once per
+    window (FP32, device inputs), (2) the reference's CUDA path called once
+    per window and (3) the reference's C library on the host cores -- (2)
+    and (3) on a sample of windows, extrapolated to the whole batch."""
     import torch
     import beampower_b200 as bp
     from beampower_b200.batch import Window, WindowBatch
@@ -616,6 +744,7 @@ def run_batch(args, local_rank):
     torch.cuda.synchronize()
     sampler.start()
     time.sleep(0.3)
+    launches0 = bp.core.launch_count()
     e0, e1 = ev(), ev()
     e0.record()
     for _ in range(args.steps):
@@ -640,28 +769,58 @@ def run_batch(args, local_rank):
         torch.cuda.synchronize()
         plain_ms.append((time.perf_counter() - t0) * 1e3)
     plain = statistics.mean(plain_ms)
+    value = terms / (ms_batch * 1e-3)
     line = {
-        "metric": "beam terms/s (src x t x sta x phase)", "value": terms / (ms_batch * 1e-3),
+        "metric": "beam terms/s (src x t x sta x phase)", "value": value,
         "unit": "beam terms/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_batch, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32" if args.storage == "fp32" else args.storage,
         "data": "synthetic",
         "config": {"workload": wl["spec"].name, "windows": len(windows),
-                   "storage": args.storage, "graph": True, "persistent_launch": True},
+                   "storage": args.storage, "graph": True, "persistent_launch": True,
+                   "kernel_config": bp.core.load_library("gpu").bp_get_kernel_config(
+                       {"fp32": 0, "bf16": 1, "fp16": 2}[args.storage], 1),
+                   "l2": "inputs of every step > L2 (features of 128 windows), no flush"},
+        "terms_per_step": terms,
+        "gpu_launches": int((bp.core.launch_count() - launches0) / max(1, args.steps)),
         "plain_per_window": {"value": terms / (plain * 1e-3), "ms_per_step": plain,
                              "storage": "fp32",
                              "note": "beampower_b200.beamform per window, device inputs"},
-        "speedup_vs_plain": plain / ms_batch,
         "clocks": clocks,
     }
+    speed = {"vs_plain_per_window": plain / ms_batch}
+    sample = list(range(0, len(windows), max(1, len(windows) // 8)))[:8]
+    if not args.no_cpu_baseline:
+        cpu = sampled_reference("batch", "cpu", sample, args.cpu_seconds)
+        if "value" in cpu:
+            cpu.update({"cores": os.cpu_count() or 1, "kind": "reference",
+                        "ms_per_step_extrapolated": terms / cpu["value"] * 1e3,
+                        "sample": f"windows {sample}, strided source subsample each, "
+                                  "reference prestack + beamform_max, extrapolated"})
+            speed["vs_reference_cpu"] = value / cpu["value"]
+        line["cpu_baseline"] = cpu
+    if not args.no_ref_gpu:
+        rg = sampled_reference("batch", "gpu", sample, 20.0)
+        if "value" in rg:
+            rg.update({"kind": "reference CUDA (beamform.cu, sm_100a build, 1 GPU) per window",
+                       "ms_per_step_extrapolated": terms / rg["value"] * 1e3,
+                       "sample": f"windows {sample}, strided source subsample each, "
+                                 "end-to-end incl. H2D, extrapolated"})
+            speed["vs_reference_gpu_per_window"] = value / rg["value"]
+        line["ref_gpu_per_window"] = rg
+    line["speedup"] = speed
     print(json.dumps(line), flush=True)
     batch.close()
 
 
 def run_serving(args, local_rank):
-    """8 networks streaming 60 s chunks, Poisson arrivals (~200 chunks/s x
-    rate_scale in total), resident tables, carry-over, continuous batching
-    under a 150 GB budget; p50/p99 chunk latency and throughput."""
+    """8 networks streaming 60 s chunks with Poisson arrivals, resident
+    tables, carried halo, continuous batching under a 150 GB budget,
+    earliest-deadline-first admission and priority streams.  Capacity is
+    estimated from each network's chunk device time alone; p50/p99 latency is
+    swept over offered loads of 5-75 % of it (overall and for the
+    400,000-source networks alone); the headline throughput is measured at
+    the specified ~200 chunks/s (beyond one GPU's capacity)."""
     import torch
     from beampower_b200.stream import NetworkStream, StreamScheduler
     from beampower_b200.synthetic import SERVING, make_serving_networks, serving_record
@@ -679,67 +838,133 @@ def run_serving(args, local_rank):
         L = n["chunk"]
         chunks[n["name"]] = [torch.from_numpy(F[:, :, i * L:(i + 1) * L].copy()).pin_memory()
                              for i in range(pool)]
-    rng = np.random.default_rng(1)
-    arrivals = []
+    large = {n["name"] for n in nets if n["delays"].shape[0] >= 400000}
+    counters = {n["name"]: 0 for n in nets}
+
+    def next_chunk(name):
+        c = chunks[name][counters[name] % pool]
+        counters[name] += 1
+        return c
+
+    # device time of one chunk per network alone (after a warm-up chunk)
+    alone_ms = {}
     for n in nets:
-        rate = n["rate"] * args.rate_scale
-        t = 0.0
-        while True:
-            t += rng.exponential(1.0 / rate)
-            if t > args.duration:
-                break
-            arrivals.append((t, n["name"]))
-    arrivals.sort()
-    # warm-up: one chunk per network
-    sched = StreamScheduler(streams, max_inflight=args.max_inflight, memory_budget=150e9)
-    for n in nets:
-        sched.submit(n["name"], chunks[n["name"]][0])
-    sched.drain()
-    torch.cuda.synchronize()
-    sched = StreamScheduler(streams, max_inflight=args.max_inflight, memory_budget=150e9)
+        ns = streams[n["name"]]
+        ns.push(next_chunk(n["name"]))
+        ns.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(ns.stream)
+        for _ in range(3):
+            ns.push(next_chunk(n["name"]))
+        e1.record(ns.stream)
+        ns.synchronize()
+        alone_ms[n["name"]] = e0.elapsed_time(e1) / 3
+    busy_per_s = sum(n["rate"] * alone_ms[n["name"]] * 1e-3 for n in nets)  # at rate_scale 1
+    cap_scale = 1.0 / busy_per_s  # rate_scale that fills one GPU
+
+    def run_load(scale, duration, max_inflight, seed):
+        for ns in streams.values():
+            ns.results = []
+        rng = np.random.default_rng(seed)
+        arrivals = []
+        for n in nets:
+            t = 0.0
+            while True:
+                t += rng.exponential(1.0 / (n["rate"] * scale))
+                if t > duration:
+                    break
+                arrivals.append((t, n["name"]))
+        arrivals.sort()
+        sched = StreamScheduler(streams, max_inflight=max_inflight, memory_budget=150e9,
+                                latency_budget=0.05)
+        t_start = time.perf_counter()
+        k = 0
+        while k < len(arrivals) or sched.pending or sched.inflight:
+            now = time.perf_counter() - t_start
+            while k < len(arrivals) and arrivals[k][0] <= now:
+                name = arrivals[k][1]
+                sched.submit(name, next_chunk(name), arrival=t_start + arrivals[k][0])
+                k += 1
+            sched.step()
+            time.sleep(5e-5)
+        st = sched.stats()
+        lat_l = np.array([c - a for nm, a, c, *_ in sched.done if nm in large])
+        st["large_p50_ms"] = float(np.percentile(lat_l, 50) * 1e3) if lat_l.size else None
+        st["large_p99_ms"] = float(np.percentile(lat_l, 99) * 1e3) if lat_l.size else None
+        st["large_chunks"] = int(lat_l.size)
+        st["offered_chunks_per_s"] = sum(n["rate"] * scale for n in nets)
+        return st
+
     sampler = ClockSampler(local_rank)
     sampler.start()
-    counters = {n["name"]: 1 for n in nets}
-    t_start = time.perf_counter()
-    k = 0
-    while k < len(arrivals) or sched.pending or sched.inflight:
-        now = time.perf_counter() - t_start
-        while k < len(arrivals) and arrivals[k][0] <= now:
-            name = arrivals[k][1]
-            sched.submit(name, chunks[name][counters[name] % pool],
-                         arrival=t_start + arrivals[k][0])
-            counters[name] += 1
-            k += 1
-        sched.step()
-        time.sleep(5e-5)
+    curve = []
+    for frac in (0.05, 0.10, 0.25, 0.50, 0.75):
+        scale = frac * cap_scale
+        duration = max(args.duration, 150.0 / (SERVING.total_rate * scale))
+        st = run_load(scale, duration, args.max_inflight, seed=int(frac * 1000))
+        curve.append({"load_of_capacity": frac, "offered_chunks_per_s": st["offered_chunks_per_s"],
+                      "chunks": st["chunks"], "duration_s": duration,
+                      "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
+                      "large_p50_ms": st["large_p50_ms"], "large_p99_ms": st["large_p99_ms"],
+                      "large_chunks": st["large_chunks"], "terms_per_s": st["terms_per_s"]})
+    st = run_load(args.rate_scale, args.duration, args.max_inflight, seed=1)
     clocks = sampler.stop()
-    st = sched.stats()
-    offered = sum(n["rate"] * args.rate_scale for n in nets)
+    ok = [c["load_of_capacity"] for c in curve
+          if c["large_p99_ms"] is not None and c["large_p99_ms"] < 50.0]
     offered_terms = sum(n["rate"] * args.rate_scale * n["delays"].shape[0] * n["chunk"]
                         * n["n_stations"] * 2 for n in nets)
+    value = st.get("terms_per_s")
     line = {
-        "metric": "beam terms/s (src x t x sta x phase)", "value": st.get("terms_per_s"),
-        "unit": "beam terms/s", "n_gpus": 1, "steps": st.get("chunks"), "warmup": len(nets),
+        "metric": "beam terms/s (src x t x sta x phase)", "value": value,
+        "unit": "beam terms/s", "n_gpus": 1, "steps": st.get("chunks"), "warmup": 4 * len(nets),
         "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32" if args.storage == "fp32" else args.storage,
         "data": "synthetic",
         "config": {"workload": SERVING.name, "networks": len(nets),
-                   "offered_chunks_per_s": offered, "offered_terms_per_s": offered_terms,
-                   "duration_s": args.duration, "max_inflight": args.max_inflight,
-                   "storage": args.storage},
+                   "offered_chunks_per_s": st["offered_chunks_per_s"],
+                   "offered_terms_per_s": offered_terms, "duration_s": args.duration,
+                   "max_inflight": args.max_inflight, "storage": args.storage,
+                   "admission": "earliest deadline first (arrival + 50 ms)",
+                   "streams": "priority pool, oldest chunk in flight highest"},
         "latency_ms": {"p50": st.get("p50_ms"), "p99": st.get("p99_ms"),
-                       "max": st.get("max_ms")},
+                       "max": st.get("max_ms"), "large_p50": st.get("large_p50_ms"),
+                       "large_p99": st.get("large_p99_ms")},
         "latency_breakdown_ms": {k: st.get(k) for k in (
             "wait_p50_ms", "wait_p99_ms", "admit_to_start_p50_ms", "admit_to_start_p99_ms",
             "device_p50_ms", "device_p99_ms")},
+        "capacity": {"chunk_device_ms_alone": alone_ms,
+                     "chunks_per_s": SERVING.total_rate * cap_scale,
+                     "of_specified_load": cap_scale,
+                     "large_networks": sorted(large)},
+        "load_curve": curve,
+        "highest_load_with_large_p99_below_50ms": max(ok) if ok else None,
         "queue": {k: st.get(k) for k in ("peak_queue_depth", "peak_inflight",
                                           "peak_device_bytes_admitted")},
         "per_network": st.get("per_network"),
         "chunks_done": st.get("chunks"), "span_s": st.get("span_s"),
         "clocks": clocks,
     }
+    sample = list(range(len(nets)))
+    speed = {}
+    if not args.no_cpu_baseline:
+        cpu = sampled_reference("serving", "cpu", sample, args.cpu_seconds)
+        if "value" in cpu:
+            cpu.update({"cores": os.cpu_count() or 1, "kind": "reference",
+                        "sample": "one 60 s chunk (+ its max-delay halo) of every network, "
+                                  "strided source subsample, reference prestack + "
+                                  "beamform_max"})
+            speed["vs_reference_cpu"] = value / cpu["value"]
+        line["cpu_baseline"] = cpu
+    if not args.no_ref_gpu:
+        rg = sampled_reference("serving", "gpu", sample, 20.0)
+        if "value" in rg:
+            rg.update({"kind": "reference CUDA (beamform.cu, sm_100a build, 1 GPU) per chunk",
+                       "sample": "one 60 s chunk (+ halo) of every network, strided source "
+                                 "subsample, end-to-end incl. H2D"})
+            speed["vs_reference_gpu_per_chunk"] = value / rg["value"]
+        line["ref_gpu_per_chunk"] = rg
+    line["speedup"] = speed
     print(json.dumps(line), flush=True)
-
 
 
 # ----------------------------------------------------------------------------
