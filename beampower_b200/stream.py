@@ -26,10 +26,10 @@ deadline first instead of sharing them evenly among all chunks in flight.
 Latency is arrival (host clock) to the completion event of the chunk's last
 kernel (device clock, mapped to the host clock once).
 """
-import heapq
 from __future__ import annotations
 
 import ctypes as ct
+import heapq
 import itertools
 import time
 

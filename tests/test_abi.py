@@ -127,3 +127,15 @@ def test_kernel_configs_described():
         assert 64 % d["sources_per_block"] == 0
         assert d["samples_per_lane"] % 2 == 0 and d["stages"] >= 2
         assert d["stations_per_stage"] in (1, 2) and d["blocks_per_sm"] >= 1
+
+
+def test_every_package_module_imports():
+    """Every module of the package imports on a machine without a GPU (the
+    GPU-only tests would otherwise be the first to see a syntax error)."""
+    import importlib
+    import pkgutil
+    import beampower_b200
+    names = [m.name for m in pkgutil.iter_modules(beampower_b200.__path__)]
+    assert "stream" in names and "batch" in names
+    for name in names:
+        importlib.import_module(f"beampower_b200.{name}")
