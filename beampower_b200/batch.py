@@ -71,7 +71,7 @@ class WindowBatch:
         trace bytes and stays within 1e-3 of a float64 beam (11 significant
         bits: at most two roundings of 2^-11 per term of one sign); FP32
         gives the reference's bits; BF16 (8 significant bits) cannot promise
-        1e-3 (one rounding alone is up to 2^-9 = 1.95e-3).
+        1e-3 (one rounding alone is up to 2^-8 = 3.9e-3).
     """
 
     def __init__(self, tables, windows, weights_phases, storage="fp16", stream=None):

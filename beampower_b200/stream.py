@@ -54,7 +54,7 @@ class NetworkStream:
     out_of_bounds: 'strict' or 'flexible'
     storage: 'fp16' (default: within 1e-3 of a float64 beam), 'fp32' (the
         reference's bits; streamed output equals the offline call bit for
-        bit) or 'bf16' (within 2e-3)
+        bit) or 'bf16' (within 4e-3)
     """
 
     def __init__(self, table: TravelTimeTable, weights_phases, out_of_bounds="strict",

@@ -7,10 +7,11 @@ each term goes through, plus FP32 accumulation (n 2^-24, below 1e-5 here):
   FP16 storage: 1e-3.  11 significant bits, unit roundoff 2^-11 = 4.9e-4;
     a term is rounded once when stored and once more in the FP16 sum of its
     phases: at most 2 x 4.9e-4 = 9.8e-4.
-  BF16 storage: 2e-3.  8 significant bits, unit roundoff 2^-9 = 1.95e-3;
+  BF16 storage: 4e-3.  8 significant bits, unit roundoff 2^-8 = 3.9e-3;
     a term is rounded once, when stored (each phase has its own FP32 FMA).
     BF16 therefore cannot promise 1e-3: a single stored value may be off by
-    1.95e-3, and beams of few terms can keep most of that.
+    3.9e-3, and beams of few terms keep much of that (measured up to 2.9e-3
+    on the small random cases, 1.7e-3 on the 4,000-source network).
 Argmax: identical wherever the float64 top-two margin exceeds the tolerance.
 """
 import numpy as np
@@ -20,7 +21,7 @@ from conftest import load_golden
 
 pytestmark = pytest.mark.gpu
 
-TOL = {"fp16": 1e-3, "bf16": 2e-3}
+TOL = {"fp16": 1e-3, "bf16": 4e-3}
 
 
 def _margin_mask(beam64, valid, tol):
