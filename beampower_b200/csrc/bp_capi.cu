@@ -333,14 +333,41 @@ int rowcap_for(const bp_table* t, int cfg) {
                               bp::kAlign);
 }
 
-// The preferred config if its shared memory fits this table, else config 0.
+int device_smem_per_sm(int dev) {
+  static int cache[64] = {0};
+  if (dev >= 0 && dev < 64 && cache[dev]) return cache[dev];
+  int v = 0;
+  cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+  if (dev >= 0 && dev < 64) cache[dev] = v;
+  return v;
+}
+
+// Config `c` serves table `t`: its shared memory fits a block, and the
+// blocks per SM it is built for fit an SM (a two-block shape left at one
+// block per SM runs at half its occupancy).
+bool config_fits(const bp_table* t, int c, int storage, bool maxred) {
+  const size_t need = staged_smem_bytes(c, t->dev.P, maxred, rowcap_for(t, c),
+                                        std::max(1, t->info.max_active), storage);
+  const int minb = cfg_of(c).minb;
+  return need <= (size_t)device_smem_optin(t->device) &&
+         (need + 1024) * (size_t)minb <= (size_t)device_smem_per_sm(t->device);
+}
+
+// Fallback order when the chosen shape does not fit a table, fastest first
+// (measured on the 400,000-source workload).
+const int kOrderF32[kNumConfigs] = {8, 3, 0, 1, 2, 4, 5, 6, 7};
+const int kOrder16[kNumConfigs] = {2, 1, 6, 7, 0, 5, 4, 3, 8};
+
+// The preferred config if it serves this table, else the first one of the
+// storage's fallback order that does; config 0 (the smallest) as the last
+// resort.
 int config_for(const bp_table* t, int storage, bool maxred) {
   const int c = pick_config(storage, maxred);
-  if (c != 0 && staged_smem_bytes(c, t->dev.P, maxred, rowcap_for(t, c),
-                                  std::max(1, t->info.max_active), storage) >
-                     (size_t)device_smem_optin(t->device))
-    return 0;
-  return c;
+  if (config_fits(t, c, storage, maxred)) return c;
+  const int* order = storage == BP_STORAGE_F32 ? kOrderF32 : kOrder16;
+  for (int i = 0; i < kNumConfigs; ++i)
+    if (config_fits(t, order[i], storage, maxred)) return order[i];
+  return 0;
 }
 
 int choose_tiles_per_chunk(int n_tt, int n_tiles, int dev) {
@@ -1126,7 +1153,7 @@ struct bp_batch {
 };
 
 namespace {
-constexpr int kBatchSamplesPerItem = 4096;  // samples per work item
+constexpr int kBatchSamplesPerItem = 16384;  // samples per work item
 
 int masked_minmax(const bp::TableView& tv, int P, const uint32_t* mask, int2* out,
                   cudaStream_t st) {
@@ -1160,10 +1187,23 @@ int bp_batch_create(const bp_table* const* tables, int n_tables, const bp_record
   BP_CUDA(cudaGetDevice(&dev));
   retain_pool(dev);
   const int P = tables[0] ? tables[0]->dev.P : 0;
-  int cfg = pick_config(storage, true);
-  for (int i = 0; i < n_tables; ++i)
-    if (tables[i] && tables[i]->info.uses_window_kernel && config_for(tables[i], storage, true) != cfg)
-      cfg = 0;
+  // the preferred shape if it serves every table, else the first of the
+  // fallback order that does
+  int cfg = -1;
+  {
+    const int pref = pick_config(storage, true);
+    const int* order = storage == BP_STORAGE_F32 ? kOrderF32 : kOrder16;
+    for (int i = -1; i < kNumConfigs && cfg < 0; ++i) {
+      const int c = i < 0 ? pref : order[i];
+      bool all = true;
+      for (int j = 0; j < n_tables; ++j)
+        if (tables[j] && tables[j]->info.uses_window_kernel &&
+            !config_fits(tables[j], c, storage, true))
+          all = false;
+      if (all) cfg = c;
+    }
+    if (cfg < 0) cfg = 0;
+  }
   const int tt = cfg_time_tile(cfg);
   int rowcap = 0, max_active = 1;
   bool any_nonfinite = false;

@@ -906,7 +906,9 @@ def run_serving(args, local_rank):
                       "chunks": st["chunks"], "duration_s": duration,
                       "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
                       "large_p50_ms": st["large_p50_ms"], "large_p99_ms": st["large_p99_ms"],
-                      "large_chunks": st["large_chunks"], "terms_per_s": st["terms_per_s"]})
+                      "large_chunks": st["large_chunks"], "terms_per_s": st["terms_per_s"],
+                      "wait_p99_ms": st["wait_p99_ms"], "device_p50_ms": st["device_p50_ms"],
+                      "device_p99_ms": st["device_p99_ms"]})
     st = run_load(args.rate_scale, args.duration, args.max_inflight, seed=1)
     clocks = sampler.stop()
     ok = [c["load_of_capacity"] for c in curve
