@@ -75,7 +75,8 @@ def _store(data):
 
 def autotune(table, traces, out_of_bounds=0, reduce="max", repeats=2, write_cache=True):
     """Time every kernel shape on (table, traces); select the fastest for the
-    traces' storage and the given reduce.  Returns {config: ms} and the choice."""
+    traces' storage and the given reduce.  Returns {config: ms} and the choice;
+    shapes whose shared memory does not fit this table are None."""
     import torch
     lib = load_library("gpu")
     storage = traces.storage
@@ -84,6 +85,9 @@ def autotune(table, traces, out_of_bounds=0, reduce="max", repeats=2, write_cach
     times = {}
     for c, _ in configs():
         check(lib.bp_set_kernel_config(storage, red, c))
+        if lib.bp_table_kernel_config(table.handle, storage, red) != c:
+            times[c] = None  # does not fit this table (another shape would run)
+            continue
         run = (lambda: table.beamform_max(traces, out_of_bounds)) if red == REDUCE_MAX else \
             (lambda: table.beamform(traces, out_of_bounds))
         run()  # warm-up (kernel attributes, lazy loading)
@@ -95,7 +99,11 @@ def autotune(table, traces, out_of_bounds=0, reduce="max", repeats=2, write_cach
         ev1.record()
         torch.cuda.synchronize()
         times[c] = ev0.elapsed_time(ev1) / repeats
-    best = min(times, key=times.get)
+    ran = {c: t for c, t in times.items() if t is not None}
+    if not ran:
+        check(lib.bp_set_kernel_config(storage, red, prev))
+        return {"times_ms": times, "best": None, "previous": prev}
+    best = min(ran, key=ran.get)
     check(lib.bp_set_kernel_config(storage, red, best))
     if write_cache:
         data = _load()

@@ -146,6 +146,7 @@ SIGNATURES = {
                                _int),
     "bp_set_kernel_config": ([_int, _int, _int], _int),
     "bp_get_kernel_config": ([_int, _int], _int),
+    "bp_table_kernel_config": ([_vp, _int, _int], _int),
     "bp_debug_wait_timeout": ([ct.c_ulonglong, _vp, ct.POINTER(_int)], _int),
     "bp_last_error": ([], ct.c_char_p),
     "bp_version": ([], ct.c_char_p),

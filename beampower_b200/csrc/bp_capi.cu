@@ -1470,6 +1470,14 @@ int bp_set_kernel_config(int storage, int reduce, int cfg) {
   return BP_OK;
 }
 
+int bp_table_kernel_config(const bp_table* t, int storage, int reduce) {
+  if (!t) return fail(BP_ERR_INVALID_ARGUMENT, "NULL table");
+  if (storage < 0 || storage > 2 || (reduce != BP_REDUCE_MAX && reduce != BP_REDUCE_NONE))
+    return fail(BP_ERR_INVALID_ARGUMENT, "bad storage / reduce");
+  if (!t->info.uses_window_kernel) return -1;
+  return config_for(t, storage, reduce == BP_REDUCE_MAX);
+}
+
 int bp_get_kernel_config(int storage, int reduce) {
   if (storage < 0 || storage > 2) return 0;
   return pick_config(storage, reduce == BP_REDUCE_MAX);

@@ -286,6 +286,7 @@ class StreamScheduler:
         self.pending = []  # heap of (deadline, seq, arrival, name, chunk)
         self.inflight = []  # (arrival, name, event, bytes, terms, admit, start event)
         self.mem_in_use = 0
+        self.push_host_s = []  # host seconds spent enqueueing each admitted chunk
         self.done = []  # (name, arrival, completion, terms)
         dev = next(iter(self.networks.values())).device
         self.device = dev
@@ -356,6 +357,7 @@ class StreamScheduler:
                 stream = self.prio_streams[min(len(self.inflight), len(self.prio_streams) - 1)]
             ev0 = torch.cuda.Event(enable_timing=True)
             net.push(chunk, stream=stream, start_event=ev0)
+            self.push_host_s.append(time.perf_counter() - admit)
             terms = (net.t_emit - t_emit0) * net.table.n_sources * net.S * net.P
             ev = torch.cuda.Event(enable_timing=True)
             ev.record(net.stream if stream is None else stream)
@@ -415,6 +417,8 @@ class StreamScheduler:
                 "wait_p50_ms": pct(wait, 50), "wait_p99_ms": pct(wait, 99),
                 "admit_to_start_p50_ms": pct(launch, 50), "admit_to_start_p99_ms": pct(launch, 99),
                 "device_p50_ms": pct(device, 50), "device_p99_ms": pct(device, 99),
+                "enqueue_p50_ms": pct(np.array(self.push_host_s), 50),
+                "enqueue_p99_ms": pct(np.array(self.push_host_s), 99),
                 "peak_queue_depth": self.peak_pending, "peak_inflight": self.peak_inflight,
                 "peak_device_bytes_admitted": self.peak_mem,
                 "cancelled": len(self.cancelled), "timed_out": len(self.timed_out),

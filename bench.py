@@ -839,6 +839,15 @@ def run_serving(args, local_rank):
         chunks[n["name"]] = [torch.from_numpy(F[:, :, i * L:(i + 1) * L].copy()).pin_memory()
                              for i in range(pool)]
     large = {n["name"] for n in nets if n["delays"].shape[0] >= 400000}
+    lib = streams[nets[0]["name"]].lib
+    st_id = {"fp32": 0, "bf16": 1, "fp16": 2}[args.storage]
+    net_info = {n["name"]: {"n_sources": int(n["delays"].shape[0]),
+                            "n_stations": n["n_stations"], "fs": n["fs"], "chunk": n["chunk"],
+                            "max_spread": streams[n["name"]].table.info["max_spread"],
+                            "max_delay": streams[n["name"]].table.info["max_delay"],
+                            "kernel_config": lib.bp_table_kernel_config(
+                                streams[n["name"]].table.handle, st_id, 1),
+                            "rate": n["rate"]} for n in nets}
     counters = {n["name"]: 0 for n in nets}
 
     def next_chunk(name):
@@ -908,7 +917,9 @@ def run_serving(args, local_rank):
                       "large_p50_ms": st["large_p50_ms"], "large_p99_ms": st["large_p99_ms"],
                       "large_chunks": st["large_chunks"], "terms_per_s": st["terms_per_s"],
                       "wait_p99_ms": st["wait_p99_ms"], "device_p50_ms": st["device_p50_ms"],
-                      "device_p99_ms": st["device_p99_ms"]})
+                      "device_p99_ms": st["device_p99_ms"],
+                      "enqueue_p50_ms": st["enqueue_p50_ms"],
+                      "enqueue_p99_ms": st["enqueue_p99_ms"]})
     st = run_load(args.rate_scale, args.duration, args.max_inflight, seed=1)
     clocks = sampler.stop()
     ok = [c["load_of_capacity"] for c in curve
@@ -933,7 +944,8 @@ def run_serving(args, local_rank):
                        "large_p99": st.get("large_p99_ms")},
         "latency_breakdown_ms": {k: st.get(k) for k in (
             "wait_p50_ms", "wait_p99_ms", "admit_to_start_p50_ms", "admit_to_start_p99_ms",
-            "device_p50_ms", "device_p99_ms")},
+            "device_p50_ms", "device_p99_ms", "enqueue_p50_ms", "enqueue_p99_ms")},
+        "networks": net_info,
         "capacity": {"chunk_device_ms_alone": alone_ms,
                      "chunks_per_s": SERVING.total_rate * cap_scale,
                      "of_specified_load": cap_scale,

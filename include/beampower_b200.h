@@ -452,6 +452,11 @@ BP_API int bp_kernel_config_shape(int config, int *stations_per_stage,
                                   int *sources_per_block, int *blocks_per_sm);
 BP_API int bp_set_kernel_config(int storage, int reduce, int config);
 BP_API int bp_get_kernel_config(int storage, int reduce);
+/* The shape a call on this table runs with (storage, reduce): the chosen one
+ * when its shared memory and blocks per SM fit the table, else the first
+ * that fits in a fixed, measured order; -1 when the table uses the direct
+ * kernel, a negative error code for bad arguments. */
+BP_API int bp_table_kernel_config(const bp_table *table, int storage, int reduce);
 
 /* ---- diagnostics -------------------------------------------------------- */
 /* Last error message of the calling thread ("" if none). */
