@@ -290,16 +290,17 @@ int launch_window(int cfg, int P, bool checked, int storage, const bp::LaunchArg
 }
 
 template <int CFG>
-size_t staged_smem_cfg(int P, bool maxred, int rowcap, int max_active, int row_factor) {
+size_t staged_smem_cfg(int P, bool maxred, int rowcap, int max_active, int row_factor,
+                       int red_rows) {
   using C = KCfg<CFG>;
   auto f = [&](auto tag) -> size_t {
     constexpr int PP = decltype(tag)::value;
     if (maxred)
       return bp::WindowSmem<PP, C::KS, C::MT, C::WS, C::NSTAGE, C::SPS, true>(
-                 rowcap, max_active, row_factor)
+                 rowcap, max_active, row_factor, red_rows)
           .total;
     return bp::WindowSmem<PP, C::KS, C::MT, C::WS, C::NSTAGE, C::SPS, false>(
-               rowcap, max_active, row_factor)
+               rowcap, max_active, row_factor, red_rows)
         .total;
   };
   switch (P) {
@@ -312,19 +313,20 @@ size_t staged_smem_cfg(int P, bool maxred, int rowcap, int max_active, int row_f
 }
 
 // Shared memory of the staged kernel; storage < 0: the largest over storages.
-size_t staged_smem_bytes(int cfg, int P, bool maxred, int rowcap, int max_active, int storage) {
+size_t staged_smem_bytes(int cfg, int P, bool maxred, int rowcap, int max_active, int storage,
+                         int red_rows) {
   const int rf = storage == BP_STORAGE_F32 ? bp::ring_row_factor<BP_STORAGE_F32>()
                                            : bp::ring_row_factor<BP_STORAGE_F16>();
   switch (cfg) {
-    case 1: return staged_smem_cfg<1>(P, maxred, rowcap, max_active, rf);
-    case 2: return staged_smem_cfg<2>(P, maxred, rowcap, max_active, rf);
-    case 3: return staged_smem_cfg<3>(P, maxred, rowcap, max_active, rf);
-    case 4: return staged_smem_cfg<4>(P, maxred, rowcap, max_active, rf);
-    case 5: return staged_smem_cfg<5>(P, maxred, rowcap, max_active, rf);
-    case 6: return staged_smem_cfg<6>(P, maxred, rowcap, max_active, rf);
-    case 7: return staged_smem_cfg<7>(P, maxred, rowcap, max_active, rf);
-    case 8: return staged_smem_cfg<8>(P, maxred, rowcap, max_active, rf);
-    default: return staged_smem_cfg<0>(P, maxred, rowcap, max_active, rf);
+    case 1: return staged_smem_cfg<1>(P, maxred, rowcap, max_active, rf, red_rows);
+    case 2: return staged_smem_cfg<2>(P, maxred, rowcap, max_active, rf, red_rows);
+    case 3: return staged_smem_cfg<3>(P, maxred, rowcap, max_active, rf, red_rows);
+    case 4: return staged_smem_cfg<4>(P, maxred, rowcap, max_active, rf, red_rows);
+    case 5: return staged_smem_cfg<5>(P, maxred, rowcap, max_active, rf, red_rows);
+    case 6: return staged_smem_cfg<6>(P, maxred, rowcap, max_active, rf, red_rows);
+    case 7: return staged_smem_cfg<7>(P, maxred, rowcap, max_active, rf, red_rows);
+    case 8: return staged_smem_cfg<8>(P, maxred, rowcap, max_active, rf, red_rows);
+    default: return staged_smem_cfg<0>(P, maxred, rowcap, max_active, rf, red_rows);
   }
 }
 
@@ -342,15 +344,27 @@ int device_smem_per_sm(int dev) {
   return v;
 }
 
-// Config `c` serves table `t`: its shared memory fits a block, and the
-// blocks per SM it is built for fit an SM (a two-block shape left at one
-// block per SM runs at half its occupancy).
-bool config_fits(const bp_table* t, int c, int storage, bool maxred) {
-  const size_t need = staged_smem_bytes(c, t->dev.P, maxred, rowcap_for(t, c),
-                                        std::max(1, t->info.max_active), storage);
+// Rows of the max buffer with which config `c` serves table `t`: one per
+// consumer warp when that fits, else a single (atomic) row; 0 when neither
+// fits a block, or the blocks per SM the shape is built for do not fit an
+// SM (a two-block shape left at one block per SM runs at half its
+// occupancy).  Without the max reduction the buffer is empty.
+int rows_for(const bp_table* t, int c, int storage, bool maxred) {
+  const int ws = cfg_of(c).ws;
   const int minb = cfg_of(c).minb;
-  return need <= (size_t)device_smem_optin(t->device) &&
-         (need + 1024) * (size_t)minb <= (size_t)device_smem_per_sm(t->device);
+  for (int rows : {ws, 1}) {
+    const size_t need = staged_smem_bytes(c, t->dev.P, maxred, rowcap_for(t, c),
+                                          std::max(1, t->info.max_active), storage, rows);
+    if (need <= (size_t)device_smem_optin(t->device) &&
+        (need + 1024) * (size_t)minb <= (size_t)device_smem_per_sm(t->device))
+      return rows;
+    if (!maxred) break;
+  }
+  return 0;
+}
+
+bool config_fits(const bp_table* t, int c, int storage, bool maxred) {
+  return rows_for(t, c, storage, maxred) > 0;
 }
 
 // Fallback order when the chosen shape does not fit a table, fastest first
@@ -431,6 +445,7 @@ int run_staged(const bp_table* t, const void* traces, int storage, const float* 
   a.tiles_per_chunk = choose_tiles_per_chunk(n_tt, n_btiles, t->device);
   a.rowcap = rowcap_for(t, cfg);
   a.max_active = std::max(1, t->info.max_active);
+  a.red_rows = std::max(1, rows_for(t, cfg, storage, maxred));
   a.status = t->status;
   if (n_tt == 0) return BP_OK;
   const long long blocks =
@@ -679,7 +694,8 @@ int bp_table_create(const int32_t* d_delays, const float* d_weights, size_t N, s
     const int rowcap = (int)bp::align_up_sz((size_t)(cfg_time_tile(0) + in.max_spread + 1),
                                             bp::kAlign);
     // sized for the largest storage, so that the choice holds for every call
-    const size_t need = staged_smem_bytes(0, (int)P, true, rowcap, std::max(1, in.max_active), -1);
+    const size_t need =
+        staged_smem_bytes(0, (int)P, true, rowcap, std::max(1, in.max_active), -1, 1);
     if (need > (size_t)device_smem_optin(t->device)) use_window = false;
   }
   in.uses_window_kernel = use_window ? 1 : 0;
@@ -1140,6 +1156,7 @@ struct bp_batch {
   int rowcap;
   int cfg;
   int max_active;
+  int red_rows;
   bool checked;
   void* mem;                        // device: tables, records, prefix, keys, srcmm, queue, status
   bp::TableView* d_tables;
@@ -1204,6 +1221,11 @@ int bp_batch_create(const bp_table* const* tables, int n_tables, const bp_record
     }
     if (cfg < 0) cfg = 0;
   }
+  // one max-buffer row per warp only if every table leaves room for it
+  int red_rows = cfg_of(cfg).ws;
+  for (int j = 0; j < n_tables; ++j)
+    if (tables[j] && tables[j]->info.uses_window_kernel)
+      red_rows = std::min(red_rows, std::max(1, rows_for(tables[j], cfg, storage, true)));
   const int tt = cfg_time_tile(cfg);
   int rowcap = 0, max_active = 1;
   bool any_nonfinite = false;
@@ -1269,6 +1291,7 @@ int bp_batch_create(const bp_table* const* tables, int n_tables, const bp_record
   b->rowcap = rowcap;
   b->cfg = cfg;
   b->max_active = max_active;
+  b->red_rows = red_rows;
   b->checked = any_flexible && any_nonfinite;
   b->stream = st;
   size_t off = 0;
@@ -1345,6 +1368,7 @@ int bp_batch_run(bp_batch* b, void* stream) {
   a.next_item = b->d_queue;
   a.rowcap = b->rowcap;
   a.max_active = b->max_active;
+  a.red_rows = b->red_rows;
   a.status = b->d_status;
   if (int rc = launch_window<true>(b->cfg, b->P, b->checked, b->storage, a, true, 0, b->device,
                                    st))
@@ -1415,6 +1439,7 @@ int bp_record_beamform_max_dev(const bp_table* t, const bp_record* q, int storag
   a.tiles_per_chunk = choose_tiles_per_chunk(n_tt, n_btiles, t->device);
   a.rowcap = rowcap_for(t, cfg);
   a.max_active = std::max(1, t->info.max_active);
+  a.red_rows = std::max(1, rows_for(t, cfg, storage, true));
   a.status = t->status;
   const long long blocks =
       (long long)((n_tt + a.tiles_per_chunk - 1) / a.tiles_per_chunk) * n_btiles;

@@ -291,6 +291,11 @@ struct LaunchArgs {
   int tiles_per_chunk;          // plain launch: time tiles per block
   int rowcap;                   // elements per ring row (per version for 16-bit)
   int max_active;
+  // Rows of the cross-warp max buffer (reduce='max'): WS, one per consumer
+  // warp (plain stores, then a max over the rows), or 1, a row the warps max
+  // into with shared-memory atomics -- the host takes 1 when the per-warp
+  // rows would not leave room for the table's ring.
+  int red_rows;
   int* status;
 };
 
@@ -308,14 +313,6 @@ struct WindowCfg {
 
 __host__ __device__ inline size_t align_up_sz(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
-// Rows of the cross-warp max buffer: one per consumer warp (plain stores,
-// then a max over the rows), or, where that would take more than 64 KB, one
-// row that the warps max into with shared-memory atomics.
-template <int WS, int TT>
-__host__ __device__ constexpr int red_rows() {
-  return (size_t)WS * TT * sizeof(unsigned long long) > 65536 ? 1 : WS;
-}
-
 // Shared-memory carve-up, used identically by host (size) and device.  A
 // ring row holds `rowcap` FP32 elements, or `rowcap` 16-bit elements of
 // each of the kHalfCopies copies; a stage holds SPS stations x P rows.
@@ -326,14 +323,14 @@ struct WindowSmem {
   static constexpr int TT = 32 * MT;
   size_t ring, meta, red, srci, st_s, st_j, st_lo, st_w, st_sc, bars, misc, total;
   // row_factor: 32-bit words per ring row per sample of capacity
-  // (ring_row_factor<STORAGE>())
-  __host__ __device__ WindowSmem(int rowcap, int max_active, int row_factor) {
+  // (ring_row_factor<STORAGE>()); red_rows: rows of the max buffer (WS or 1)
+  __host__ __device__ WindowSmem(int rowcap, int max_active, int row_factor, int red_rows) {
     size_t o = 0;
     ring = o;        o += (size_t)NSTAGE * SPS * P * rowcap * 4 * row_factor;
     o = align_up_sz(o, 16);
     meta = o;        o += (size_t)max_active * K * sizeof(M);
     o = align_up_sz(o, 16);
-    red = o;         o += MAXRED ? (size_t)red_rows<WS, TT>() * TT * sizeof(unsigned long long) : 0;
+    red = o;         o += MAXRED ? (size_t)red_rows * TT * sizeof(unsigned long long) : 0;
     o = align_up_sz(o, 16);
     srci = o;        o += (size_t)K * sizeof(int4);
     st_s = o;        o += (size_t)max_active * sizeof(int);
@@ -460,11 +457,13 @@ struct Staged {
     volatile int* abort_flag;
     int* n_act;
     int4* cur_item;
+    int red_rows;
   };
 
-  __device__ static Smem carve(unsigned char* smem, int rowcap, int max_active) {
-    const WindowSmem<P, KS, MT, WS, NSTAGE, SPS, MAXRED> L(rowcap, max_active, RF);
+  __device__ static Smem carve(unsigned char* smem, int rowcap, int max_active, int red_rows) {
+    const WindowSmem<P, KS, MT, WS, NSTAGE, SPS, MAXRED> L(rowcap, max_active, RF, red_rows);
     Smem s;
+    s.red_rows = red_rows;
     s.ring = smem + L.ring;
     s.meta_s = reinterpret_cast<M*>(smem + L.meta);
     s.red = reinterpret_cast<unsigned long long*>(smem + L.red);
@@ -540,7 +539,7 @@ struct Staged {
         if (w > rowcap) atomicOr(status, kStatusBadWindow);
       }
     }
-    if constexpr (MAXRED && red_rows<WS, TT>() == 1)
+    if (MAXRED && sm.red_rows == 1)
       for (int i = tid; i < TT; i += blockDim.x) sm.red[i] = 0ull;
     {
       // Per source slot: {source, first, end, 0} with [first, end) the
@@ -748,13 +747,13 @@ struct Staged {
         // index among equal maxima; seeding with -FLT_MAX makes NaN and
         // -FLT_MAX (and below) lose, as in the reference's running max.
         // Samples outer, so that each pair's accumulators die after use.
-        constexpr int kRows = red_rows<WS, TT>();
+        const bool one_row = sm.red_rows == 1;  // block-uniform
         // the key of sample (q, h) into this warp's row of the max buffer, or
         // into the single shared row (zero on entry) by an atomic max
         auto put = [&](int q, int h, float bv, int bi) {
           const int i = pair_sample<STORAGE>(lane, q, h);
           const unsigned long long key = bi >= 0 ? make_key(bv, bi) : 0ull;
-          if constexpr (kRows == WS) sm.red[warp * TT + i] = key;
+          if (!one_row) sm.red[warp * TT + i] = key;
           else if (key) atomicMax(&sm.red[i], key);
         };
         bool all_kept = true;  // warp-uniform: every slot keeps the whole tile
@@ -802,12 +801,16 @@ struct Staged {
         named_barrier_sync(1, NCONS);
         for (int i = tid; i < TT; i += NCONS) {
           unsigned long long b = 0ull;
+          if (one_row) {
+            b = sm.red[i];
+            sm.red[i] = 0ull;  // zero again for the next tile
+          } else {
 #pragma unroll
-          for (int w = 0; w < kRows; ++w) {
-            const unsigned long long v = sm.red[w * TT + i];
-            b = v > b ? v : b;
+            for (int w = 0; w < WS; ++w) {
+              const unsigned long long v = sm.red[w * TT + i];
+              b = v > b ? v : b;
+            }
           }
-          if constexpr (kRows == 1) sm.red[i] = 0ull;  // zero again for the next tile
           const int t = t0 + i;
           if (b != 0ull && t >= rc.out0 && t < rc.out1) red_max_u64(&rc.keys[t - rc.out0], b);
         }
@@ -1059,7 +1062,7 @@ __global__ void __launch_bounds__((WS + 1) * 32, MINB)
 beam_window_kernel(const LaunchArgs a) {
   using St = Staged<P, KS, MT, WS, NSTAGE, SPS, MAXRED, CHECKED, STORAGE>;
   extern __shared__ __align__(128) unsigned char smem[];
-  const typename St::Smem sm = St::carve(smem, a.rowcap, a.max_active);
+  const typename St::Smem sm = St::carve(smem, a.rowcap, a.max_active, a.red_rows);
   if (threadIdx.x == 0) St::init_barriers(sm);
   __syncthreads();
   const int n_btiles = a.tab0.n_tiles * St::H;
@@ -1084,7 +1087,7 @@ __global__ void __launch_bounds__((WS + 1) * 32, MINB)
 beam_batch_kernel(const LaunchArgs a) {
   using St = Staged<P, KS, MT, WS, NSTAGE, SPS, MAXRED, CHECKED, STORAGE>;
   extern __shared__ __align__(128) unsigned char smem[];
-  const typename St::Smem sm = St::carve(smem, a.rowcap, a.max_active);
+  const typename St::Smem sm = St::carve(smem, a.rowcap, a.max_active, a.red_rows);
   if (threadIdx.x == 0) St::init_barriers(sm);
   __syncthreads();
   int it = 0;

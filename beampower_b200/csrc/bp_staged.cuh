@@ -14,7 +14,7 @@ int launch_window_p(const bp::LaunchArgs& a, bool batch, long long plain_blocks,
                     cudaStream_t st) {
   using C = KCfg<CFG>;
   using L = bp::WindowSmem<P, C::KS, C::MT, C::WS, C::NSTAGE, C::SPS, MAXRED>;
-  const L lay(a.rowcap, a.max_active, bp::ring_row_factor<STORAGE>());
+  const L lay(a.rowcap, a.max_active, bp::ring_row_factor<STORAGE>(), a.red_rows);
   if (lay.total > (size_t)device_smem_optin(dev))
     return fail(BP_ERR_UNSUPPORTED, "staged kernel needs %zu B of shared memory", lay.total);
   // 16-bit storage addresses ring rows with 16-bit byte offsets

@@ -196,3 +196,27 @@ def test_fp16_factor_paths_agree(cuda, bplib):
                                   b1.view(np.uint32)), (c, oob)
     t1.close()
     t2.close()
+
+
+def test_wide_windows_fall_back_correctly(cuda, bplib, oracle_lib):
+    """Delay windows of ~2,600 samples: the 16-warp shapes keep a single
+    atomic row for the cross-warp max (the per-warp rows would not leave room
+    for the ring) and shapes that do not fit at all hand over to one that
+    does; every choice stays bit for bit equal to the oracle."""
+    from beampower_b200.tables import TravelTimeTable
+    F, A, D, W = _network(50, S=6, N=300, T=6000, unit=False, spread=2600)
+    U = oracle_lib.prestack(F, A)
+    ref = oracle_lib.beamform_max(U, D, W, 0)
+    table = TravelTimeTable(D, W)
+    assert table.info["max_spread"] > 2000
+    tr = table.traces_from_features(F, A, storage="fp32")
+    used = set()
+    for c in _configs(bplib):
+        def run():
+            used.add(bplib.bp_table_kernel_config(table.handle, 0, 1))
+            return _run(table, tr, 0, "max")
+        bm, am = _with_config(bplib, 0, "max", c, run)
+        assert np.array_equal(bm.view(np.uint32), ref[0].view(np.uint32)), c
+        assert np.array_equal(am, ref[1]), c
+    assert {1, 2, 8} & used  # a 16-warp shape ran (with the single atomic row)
+    table.close()
