@@ -287,6 +287,7 @@ class StreamScheduler:
         self.inflight = []  # (arrival, name, event, bytes, terms, admit, start event)
         self.mem_in_use = 0
         self.push_host_s = []  # host seconds spent enqueueing each admitted chunk
+        self._free, self._free_t = 0, -1.0  # cached free device memory
         self.done = []  # (name, arrival, completion, terms)
         dev = next(iter(self.networks.values())).device
         self.device = dev
@@ -346,8 +347,8 @@ class StreamScheduler:
                 continue
             net = self.networks[name]
             need = net.bytes_per_chunk(int(chunk.shape[2]))
-            free, _ = torch.cuda.mem_get_info(self.device)
-            if self.inflight and (self.mem_in_use + need > self.memory_budget or need > free):
+            if self.inflight and (self.mem_in_use + need > self.memory_budget or
+                                  need > self._free_bytes()):
                 break  # wait for memory to free up
             heapq.heappop(self.pending)
             admit = time.perf_counter()
@@ -363,6 +364,15 @@ class StreamScheduler:
             ev.record(net.stream if stream is None else stream)
             self.inflight.append((arrival, name, ev, need, terms, admit, ev0))
             self.mem_in_use += need
+
+    def _free_bytes(self):
+        """The device's free memory, queried at most every 250 ms (the query
+        takes driver locks that can stall the request loop)."""
+        now = time.perf_counter()
+        if now - self._free_t > 0.25:
+            self._free, _ = torch.cuda.mem_get_info(self.device)
+            self._free_t = now
+        return self._free
 
     def _retire(self):
         keep = []

@@ -821,6 +821,11 @@ def run_serving(args, local_rank):
     swept over offered loads of 5-75 % of it (overall and for the
     400,000-source networks alone); the headline throughput is measured at
     the specified ~200 chunks/s (beyond one GPU's capacity)."""
+    # A serving process loads every kernel when CUDA starts, so that no
+    # request pays a module load (lazy loading, torch's default, loaded a
+    # kernel on first use inside a request: tens of ms).  Read at CUDA
+    # initialisation, which has not happened yet in this process.
+    os.environ["CUDA_MODULE_LOADING"] = "EAGER"
     import torch
     from beampower_b200.stream import NetworkStream, StreamScheduler
     from beampower_b200.synthetic import SERVING, make_serving_networks, serving_record
@@ -938,6 +943,7 @@ def run_serving(args, local_rank):
                    "offered_terms_per_s": offered_terms, "duration_s": args.duration,
                    "max_inflight": args.max_inflight, "storage": args.storage,
                    "admission": "earliest deadline first (arrival + 50 ms)",
+                   "module_loading": os.environ.get("CUDA_MODULE_LOADING"),
                    "streams": "priority pool, oldest chunk in flight highest"},
         "latency_ms": {"p50": st.get("p50_ms"), "p99": st.get("p99_ms"),
                        "max": st.get("max_ms"), "large_p50": st.get("large_p50_ms"),
