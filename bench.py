@@ -699,6 +699,14 @@ def main():
         run_batch(args, local_rank)
         return
     if args.workload == "serving":
+        # A serving process loads every kernel when CUDA starts, so that no
+        # request pays a module load (with lazy loading, torch's default, a
+        # kernel used for the first time inside a request stalled it for
+        # tens of ms).  The variable is read when the process starts CUDA:
+        # restart with it set.
+        if os.environ.get("CUDA_MODULE_LOADING") != "EAGER":
+            os.environ["CUDA_MODULE_LOADING"] = "EAGER"
+            os.execv(sys.executable, [sys.executable] + sys.argv)
         run_serving(args, local_rank)
         return
     if args.workload == "stages":
@@ -821,11 +829,7 @@ def run_serving(args, local_rank):
     swept over offered loads of 5-75 % of it (overall and for the
     400,000-source networks alone); the headline throughput is measured at
     the specified ~200 chunks/s (beyond one GPU's capacity)."""
-    # A serving process loads every kernel when CUDA starts, so that no
-    # request pays a module load (lazy loading, torch's default, loaded a
-    # kernel on first use inside a request: tens of ms).  Read at CUDA
-    # initialisation, which has not happened yet in this process.
-    os.environ["CUDA_MODULE_LOADING"] = "EAGER"
+    import gc
     import torch
     from beampower_b200.stream import NetworkStream, StreamScheduler
     from beampower_b200.synthetic import SERVING, make_serving_networks, serving_record
@@ -891,6 +895,8 @@ def run_serving(args, local_rank):
         arrivals.sort()
         sched = StreamScheduler(streams, max_inflight=max_inflight, memory_budget=150e9,
                                 latency_budget=0.05)
+        gc.collect()
+        gc.disable()  # no collector pauses inside the request loop
         t_start = time.perf_counter()
         k = 0
         while k < len(arrivals) or sched.pending or sched.inflight:
@@ -901,6 +907,7 @@ def run_serving(args, local_rank):
                 k += 1
             sched.step()
             time.sleep(5e-5)
+        gc.enable()
         st = sched.stats()
         lat_l = np.array([c - a for nm, a, c, *_ in sched.done if nm in large])
         st["large_p50_ms"] = float(np.percentile(lat_l, 50) * 1e3) if lat_l.size else None
