@@ -248,6 +248,31 @@ class NetworkStream:
         return bm, am
 
 
+_PRIORITY_STREAMS = {}  # device index -> [torch.cuda.Stream], highest priority first
+
+
+def priority_streams(device):
+    """This process's pool of CUDA streams of distinct priorities on
+    `device`, highest first (priorities beyond the device's range are clamped
+    by CUDA, so the pool stops at a repeat).  Shared by every scheduler: the
+    caching allocator keeps its blocks per stream, so reused streams keep
+    their warmed-up memory."""
+    dev = torch.device(device)
+    idx = dev.index if dev.index is not None else torch.cuda.current_device()
+    pool = _PRIORITY_STREAMS.get(idx)
+    if pool is None:
+        pool, seen = [], set()
+        for k in range(16):
+            st = torch.cuda.Stream(device=idx, priority=-k)
+            if st.priority in seen:
+                break
+            seen.add(st.priority)
+            pool.append(st)
+        pool.sort(key=lambda st: st.priority)
+        _PRIORITY_STREAMS[idx] = pool
+    return pool
+
+
 class StreamScheduler:
     """Continuous batching of chunks from many networks.
 
@@ -291,24 +316,26 @@ class StreamScheduler:
         self.done = []  # (name, arrival, completion, terms)
         dev = next(iter(self.networks.values())).device
         self.device = dev
-        # streams of distinct priorities, highest first (priorities outside the
-        # device's range are clamped by CUDA, so the pool stops at a repeat)
-        self.prio_streams = []
-        if priorities:
-            seen = set()
-            for k in range(16):
-                st = torch.cuda.Stream(device=dev, priority=-k)
-                if st.priority in seen:
-                    break
-                seen.add(st.priority)
-                self.prio_streams.append(st)
-            self.prio_streams.sort(key=lambda st: st.priority)
+        self.prio_streams = priority_streams(dev) if priorities else []
         # device clock -> host clock
         torch.cuda.synchronize(dev)
         self._ev0 = torch.cuda.Event(enable_timing=True)
         self._ev0.record(torch.cuda.current_stream(dev))
         torch.cuda.synchronize(dev)
         self._host0 = time.perf_counter()
+
+    def warm_up(self, chunks):
+        """Push one chunk of every network (`chunks`: name -> chunk) through
+        every stream this scheduler may use, so that the first requests find
+        the memory they need already cached for each stream (a first
+        allocation on a stream can wait for the work running on the GPU).
+        The chunks continue each network's stream; synchronises."""
+        targets = self.prio_streams or [None]
+        for name, chunk in chunks.items():
+            for s in targets:
+                self.networks[name].push(chunk, stream=s)
+        for net in self.networks.values():
+            net.synchronize()
 
     def submit(self, name, chunk, arrival=None):
         if name not in self.networks:

@@ -916,6 +916,10 @@ def run_serving(args, local_rank):
         st["offered_chunks_per_s"] = sum(n["rate"] * scale for n in nets)
         return st
 
+    # every network's chunk once through every priority stream (cached memory
+    # per stream), then a short run at half the capacity, both untimed
+    StreamScheduler(streams).warm_up({n["name"]: next_chunk(n["name"]) for n in nets})
+    run_load(0.5 * cap_scale, 1.0, args.max_inflight, seed=7)
     sampler = ClockSampler(local_rank)
     sampler.start()
     curve = []
