@@ -9,6 +9,7 @@
 #include <atomic>
 #include <cstdint>
 #include <limits>
+#include <string>
 
 #include <cuda_runtime.h>
 #include <nvtx3/nvToolsExt.h>
@@ -20,6 +21,9 @@ namespace bp_host {
 
 // Records a printf-style message for bp_last_error() and returns code.
 int fail(int code, const char* fmt, ...);
+// The calling thread's last error message (cleared at the start of an entry
+// point, set by fail()).
+extern thread_local std::string g_last_error;
 // Maps a CUDA error to BP_ERR_OUT_OF_MEMORY / BP_ERR_CUDA with its text.
 int cuda_fail(cudaError_t e, const char* what);
 // Kernels launched by the library (bp_launch_count()).

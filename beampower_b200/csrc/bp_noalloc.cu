@@ -28,6 +28,11 @@
 
 #include "beampower_b200.h"
 #include "bp_common.cuh"
+// error recording, launch counting and NVTX ranges shared with the other
+// entry points (template kernels only: the library's other kernels are
+// defined in bp_capi.cu)
+#define BP_TEMPLATE_KERNELS_ONLY
+#include "bp_host.h"
 
 namespace {
 
@@ -42,8 +47,10 @@ constexpr int kMaxDevices = 64;
 std::mutex g_setup_mutex;
 void* g_scratch_addr[kMaxDevices] = {nullptr};
 
-// Status with the reason kept next to the check (the codes are the header's).
-inline int noalloc_fail(int code, const char* /*reason*/) { return code; }
+// Records the reason for bp_last_error() and returns the status code.
+inline int noalloc_fail(int code, const char* reason) {
+  return bp_host::fail(code, "bp_beamform_max_noalloc: %s", reason);
+}
 
 // Device address of g_scratch on the current device (set up once per device).
 int scratch_on_current_device(void** out) {
@@ -137,6 +144,8 @@ extern "C" BP_API int bp_beamform_max_noalloc(const float* d_traces, size_t n_sa
                                               size_t n_stations, size_t n_phases,
                                               int out_of_bounds, float* d_beam_max,
                                               int32_t* d_argmax, void* stream) {
+  BP_NVTX("bp_beamform_max_noalloc");
+  bp_host::g_last_error.clear();
   if (n_samples > kMaxSamples)
     return noalloc_fail(BP_ERR_SCRATCH_LIMIT,
                         "n_samples exceeds the fixed scratch limit of 524288 samples");
@@ -161,21 +170,21 @@ extern "C" BP_API int bp_beamform_max_noalloc(const float* d_traces, size_t n_sa
   const int T = (int)n_samples, N = (int)n_sources, S = (int)n_stations, P = (int)n_phases;
 
   // the previous call's keys are still in the array: clear this call's range
-  if (cudaMemsetAsync(keys, 0, n_samples * sizeof(unsigned long long), st) != cudaSuccess)
-    return noalloc_fail(BP_ERR_CUDA, "clearing the scratch keys failed");
+  BP_CUDA(cudaMemsetAsync(keys, 0, n_samples * sizeof(unsigned long long), st));
   if (N > 0) {
     noalloc_minmax_kernel<<<(unsigned)((N + 255) / 256), 256, 0, st>>>(
         d_time_delays, d_weights_sources, N, S, P, minmax);
+    BP_LAUNCHED("noalloc_minmax_kernel");
     int src_per_block = 64;
     unsigned gy = (unsigned)((N + src_per_block - 1) / src_per_block);
     dim3 grid((unsigned)((T + 255) / 256), gy);
     noalloc_direct_max_kernel<<<grid, 256, 0, st>>>(d_traces, (long long)pitch, (int)lpad, T,
                                                      d_time_delays, d_weights_sources, minmax, N,
                                                      S, P, out_of_bounds, src_per_block, keys);
+    BP_LAUNCHED("noalloc_direct_max_kernel");
   }
   noalloc_decode_kernel<<<(unsigned)((T + 255) / 256), 256, 0, st>>>(keys, T, d_beam_max,
                                                                      d_argmax);
-  if (cudaGetLastError() != cudaSuccess)
-    return noalloc_fail(BP_ERR_CUDA, "kernel launch failed");
+  BP_LAUNCHED("noalloc_decode_kernel");
   return BP_OK;
 }
