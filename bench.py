@@ -57,10 +57,13 @@ def parse():
     ap.add_argument("--storage", default=None, choices=["fp32", "bf16", "fp16"],
                     help="trace storage (default: fp32 for the large workload, fp16 for "
                          "batch and serving)")
-    ap.add_argument("--workload", default="large", choices=["large", "batch", "serving", "stages"],
+    ap.add_argument("--workload", default="large",
+                    choices=["large", "batch", "serving", "stages", "shapes"],
                     help="large: the 400k-source plain call (default); batch: 128 windows "
                          "in one persistent launch vs one call per window; serving: "
-                         "8 streamed networks with Poisson chunk arrivals")
+                         "8 streamed networks with Poisson chunk arrivals; stages: the "
+                         "tutorial's steps either side; shapes: every kernel shape timed by "
+                         "the autotuner on the 400k table and on a 50k batch table")
     ap.add_argument("--windows", type=int, default=128, help="batch workload: windows")
     ap.add_argument("--duration", type=float, default=3.0,
                     help="serving workload: seconds of arrivals")
@@ -712,6 +715,9 @@ def main():
     if args.workload == "stages":
         run_stages(args, local_rank)
         return
+    if args.workload == "shapes":
+        run_shapes(args, local_rank)
+        return
     if args.sharded:
         run_sharded(args, rank, world, local_rank)
         return
@@ -778,6 +784,27 @@ def run_batch(args, local_rank):
         plain_ms.append((time.perf_counter() - t0) * 1e3)
     plain = statistics.mean(plain_ms)
     value = terms / (ms_batch * 1e-3)
+    # the same batch with the other trace storages (CUDA graph replay, 2 steps)
+    variants = {}
+    for stg in ("fp32", "fp16", "bf16"):
+        if stg == args.storage:
+            continue
+        vb = WindowBatch(tables, windows, wl["weights_phases"], storage=stg)
+        for i in range(len(windows)):
+            vb.set_features(i, batch.features[i])
+        vb.capture()
+        vb.run()
+        torch.cuda.synchronize()
+        v0, v1 = ev(), ev()
+        v0.record()
+        for _ in range(2):
+            vb.run()
+        v1.record()
+        torch.cuda.synchronize()
+        vms = v0.elapsed_time(v1) / 2
+        variants[stg] = {"ms_per_step": vms, "value": terms / (vms * 1e-3),
+                         "vs_plain_per_window": plain / vms}
+        vb.close()
     line = {
         "metric": "beam terms/s (src x t x sta x phase)", "value": value,
         "unit": "beam terms/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
@@ -790,6 +817,7 @@ def run_batch(args, local_rank):
                        {"fp32": 0, "bf16": 1, "fp16": 2}[args.storage], 1),
                    "l2": "inputs of every step > L2 (features of 128 windows), no flush"},
         "terms_per_step": terms,
+        "storage_variants": variants,
         "gpu_launches": int((bp.core.launch_count() - launches0) / max(1, args.steps)),
         "plain_per_window": {"value": terms / (plain * 1e-3), "ms_per_step": plain,
                              "storage": "fp32",
@@ -996,6 +1024,55 @@ def run_serving(args, local_rank):
         line["ref_gpu_per_chunk"] = rg
     line["speedup"] = speed
     print(json.dumps(line), flush=True)
+
+
+def run_shapes(args, local_rank):
+    """Kernel time of every compiled shape of the staged kernel, per trace
+    storage, through the autotuner (beampower_b200.autotune): on the
+    400,000-source table of the large workload (60 stations, 180,000
+    samples) and on the 50,000-source grid of the batch workload (100
+    stations) with one 90,000-sample window over all stations.  Shapes whose
+    shared memory does not fit a table are reported as None."""
+    import torch
+    from beampower_b200 import autotune
+    from beampower_b200.core import load_library
+    from beampower_b200.synthetic import (make_batch_workload, window_features,
+                                          nominal_terms)
+    from beampower_b200.tables import TravelTimeTable
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    lib = load_library("gpu")
+    os.environ.setdefault(autotune.CACHE_ENV, os.path.join("/tmp", "bp_shapes_cache.json"))
+    wl = make_workload(LARGE)
+    bw = make_batch_workload(n_windows=1)
+    D50, W50 = bw["grids"][1]
+    F50 = window_features({**bw, "windows": [{**bw["windows"][0], "table": 1,
+                                               "n_samples": 90000, "events": []}]}, 0)
+    cases = [("large-400k-src-60-sta-180000-samples", wl["time_delays"], wl["weights_sources"],
+              wl["waveform_features"], wl["weights_phases"]),
+             ("batch-grid-50k-src-100-sta-90000-samples", D50, W50, F50, bw["weights_phases"])]
+    out = {"shapes": dict(autotune.configs()), "tables": {}}
+    sampler = ClockSampler(local_rank)
+    sampler.start()
+    for name, D, W, F, A in cases:
+        table = TravelTimeTable(D, W, device=dev)
+        N, S, P = D.shape
+        terms = nominal_terms(N, F.shape[2], S, P)
+        res = {"terms": terms, "max_spread": table.info["max_spread"],
+               "max_active": table.info["max_active"], "storages": {}}
+        for stg in ("fp32", "fp16", "bf16"):
+            tr = table.traces_from_features(F, A, storage=stg)
+            r = autotune.autotune(table, tr, repeats=2, write_cache=False)
+            res["storages"][stg] = {"ms": r["times_ms"], "best": r["best"]}
+            lib.bp_set_kernel_config(tr.storage, 1, -1)
+            res["storages"][stg]["default"] = lib.bp_table_kernel_config(
+                table.handle, tr.storage, 1)
+            del tr
+        out["tables"][name] = res
+        table.close()
+    out["clocks"] = sampler.stop()
+    print(json.dumps({"workload": "shapes", "n_gpus": 1, "data": "synthetic", **out}),
+          flush=True)
 
 
 # ----------------------------------------------------------------------------
