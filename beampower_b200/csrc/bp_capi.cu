@@ -90,8 +90,7 @@ constexpr CfgDesc cfg_desc() {
 }
 constexpr CfgDesc kCfgDesc[kNumConfigs] = {cfg_desc<0>(), cfg_desc<1>(), cfg_desc<2>(),
                                            cfg_desc<3>(), cfg_desc<4>(), cfg_desc<5>(),
-                                           cfg_desc<6>(), cfg_desc<7>(), cfg_desc<8>(),
-                                           cfg_desc<9>(), cfg_desc<10>()};
+                                           cfg_desc<6>(), cfg_desc<7>(), cfg_desc<8>()};
 
 inline const CfgDesc& cfg_of(int cfg) {
   return kCfgDesc[(cfg >= 0 && cfg < kNumConfigs) ? cfg : 0];
@@ -286,8 +285,6 @@ int launch_window(int cfg, int P, bool checked, int storage, const bp::LaunchArg
     case 6: return launch_window_c<6, MAXRED>(P, checked, storage, a, batch, blocks, dev, st);
     case 7: return launch_window_c<7, MAXRED>(P, checked, storage, a, batch, blocks, dev, st);
     case 8: return launch_window_c<8, MAXRED>(P, checked, storage, a, batch, blocks, dev, st);
-    case 9: return launch_window_c<9, MAXRED>(P, checked, storage, a, batch, blocks, dev, st);
-    case 10: return launch_window_c<10, MAXRED>(P, checked, storage, a, batch, blocks, dev, st);
     default: return launch_window_c<0, MAXRED>(P, checked, storage, a, batch, blocks, dev, st);
   }
 }
@@ -329,8 +326,6 @@ size_t staged_smem_bytes(int cfg, int P, bool maxred, int rowcap, int max_active
     case 6: return staged_smem_cfg<6>(P, maxred, rowcap, max_active, rf, red_rows);
     case 7: return staged_smem_cfg<7>(P, maxred, rowcap, max_active, rf, red_rows);
     case 8: return staged_smem_cfg<8>(P, maxred, rowcap, max_active, rf, red_rows);
-    case 9: return staged_smem_cfg<9>(P, maxred, rowcap, max_active, rf, red_rows);
-    case 10: return staged_smem_cfg<10>(P, maxred, rowcap, max_active, rf, red_rows);
     default: return staged_smem_cfg<0>(P, maxred, rowcap, max_active, rf, red_rows);
   }
 }
@@ -374,8 +369,8 @@ bool config_fits(const bp_table* t, int c, int storage, bool maxred) {
 
 // Fallback order when the chosen shape does not fit a table, fastest first
 // (measured on the 400,000-source workload).
-const int kOrderF32[kNumConfigs] = {8, 3, 0, 10, 1, 2, 9, 4, 5, 6, 7};
-const int kOrder16[kNumConfigs] = {2, 9, 1, 6, 7, 0, 5, 4, 3, 8, 10};
+const int kOrderF32[kNumConfigs] = {8, 3, 0, 1, 2, 4, 5, 6, 7};
+const int kOrder16[kNumConfigs] = {2, 1, 6, 7, 0, 5, 4, 3, 8};
 
 // The preferred config if it serves this table, else the first one of the
 // storage's fallback order that does; config 0 (the smallest) as the last

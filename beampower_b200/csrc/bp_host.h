@@ -56,8 +56,6 @@ constexpr long long kMaxInt = std::numeric_limits<int>::max();
 //   4: 16 x 2, MT 32, SPS 1, 1/SM    5: 16 x 2, MT 32, SPS 2, 1/SM
 //   6: 8 x 8, MT 16, SPS 2, 1/SM     7: 8 x 8, MT 16, SPS 1, 1/SM
 //   8: 16 x 2, MT 16, SPS 2, 1/SM (32 sources per block)
-//   9, 10: configs 2 and 8 without the producer warp (consumer warp 0 refills
-//          the ring): 16 warps, 128 registers per thread
 // Registers: a sub-partition holds 16K; 17 warps (16 consumers + producer)
 // or 2 x 9 warps put 5 warps on one sub-partition and cap a thread at 96
 // registers, 9 warps at one block per SM allow 168 (configs 6 and 7: 8 x 16
@@ -67,13 +65,11 @@ constexpr long long kMaxInt = std::numeric_limits<int>::max();
 #ifndef BP_NSTAGE
 #define BP_NSTAGE 4
 #endif
-template <int WS_, int KS_, int MT_, int SPS_, int MINB_, bool INL_ = false>
+template <int WS_, int KS_, int MT_, int SPS_, int MINB_>
 struct KShape {
   static constexpr int WS = WS_, KS = KS_, MT = MT_, SPS = SPS_, MINB = MINB_;
-  static constexpr bool INL = INL_;  // ring refilled by consumer warp 0, no producer warp
   static constexpr int NSTAGE = BP_NSTAGE;
   static constexpr int K = WS * KS;  // sources per block
-  static constexpr int THREADS = (WS + (INL ? 0 : 1)) * 32;
 };
 template <int ID> struct KCfg;
 template <> struct KCfg<0> : KShape<8, 8, 8, 1, 2> {};
@@ -85,9 +81,7 @@ template <> struct KCfg<5> : KShape<16, 2, 32, 2, 1> {};
 template <> struct KCfg<6> : KShape<8, 8, 16, 2, 1> {};
 template <> struct KCfg<7> : KShape<8, 8, 16, 1, 1> {};
 template <> struct KCfg<8> : KShape<16, 2, 16, 2, 1> {};
-template <> struct KCfg<9> : KShape<16, 4, 16, 2, 1, true> {};
-template <> struct KCfg<10> : KShape<16, 2, 16, 2, 1, true> {};
-constexpr int kNumConfigs = 11;
+constexpr int kNumConfigs = 9;
 constexpr int kTileSources = bp::kTableTile;
 
 // Launches the staged kernel of config CFG (plain grid of `blocks` blocks, or
@@ -111,8 +105,6 @@ BP_EXTERN_CFG(5)
 BP_EXTERN_CFG(6)
 BP_EXTERN_CFG(7)
 BP_EXTERN_CFG(8)
-BP_EXTERN_CFG(9)
-BP_EXTERN_CFG(10)
 #undef BP_EXTERN_CFG
 
 }  // namespace bp_host

@@ -416,13 +416,10 @@ __device__ __forceinline__ bool pack_factor16(float c, uint32_t* packed) {
 // tile is one table tile (WS * KS == kTableTile) or a part of one: block
 // tile b covers sources (b % H) * K .. + K - 1 of table tile b / H.  A ring
 // stage carries SPS consecutive active stations (one mbarrier round trip per
-// SPS stations).  INL: no producer warp; consumer warp 0 refills the ring
-// itself between its own stages (non-blocking), so a 16-warp block keeps
-// 128 registers per thread instead of the 96 of a 17-warp block.
+// SPS stations).
 template <int P, int KS, int MT, int WS, int NSTAGE, int SPS, bool MAXRED, bool CHECKED,
-          int STORAGE, bool INL = false>
+          int STORAGE>
 struct Staged {
-  static constexpr int kThreads = (WS + (INL ? 0 : 1)) * 32;
   static_assert(MT % 2 == 0 && KS % 2 == 0, "packed pairs");
   static_assert(!(CHECKED && STORAGE != BP_STORAGE_F32), "checked variant is FP32 only");
   using M = typename MetaT<P>::type;
@@ -621,7 +618,7 @@ struct Staged {
     const int n_stages = (tau1 - tau0) * n_grp;
 
     // ---- producer warp ----------------------------------------------------
-    if (!INL && warp == WS) {
+    if (warp == WS) {
       if (lane == 0) {
         const unsigned char* tr = reinterpret_cast<const unsigned char*>(rc.traces);
         int issued = 0;
@@ -697,108 +694,26 @@ struct Staged {
 
     // ---- consumer warps ---------------------------------------------------
     if constexpr (F32) {
-      consume<false>(sm, tb, rc, tau0, tau1, n_active, n_grp, rowcap, status, it0);
+      consume<false>(sm, rc, tau0, tau1, n_active, n_grp, rowcap, status, it0);
     } else {
-      if (fast16) consume<true>(sm, tb, rc, tau0, tau1, n_active, n_grp, rowcap, status, it0);
-      else consume<false>(sm, tb, rc, tau0, tau1, n_active, n_grp, rowcap, status, it0);
+      if (fast16) consume<true>(sm, rc, tau0, tau1, n_active, n_grp, rowcap, status, it0);
+      else consume<false>(sm, rc, tau0, tau1, n_active, n_grp, rowcap, status, it0);
     }
     return n_stages;
-  }
-
-  // INL, warp 0 (all lanes): issue, in order from stage `issued` on, every
-  // stage of the item whose ring slot all consumer warps have released --
-  // without waiting for a slot that is still in use.  One lane arms the
-  // stage's full barrier with the byte count, then the warp's lanes issue
-  // the stage's bulk copies (one copy per lane).
-  __device__ static void pump(const Smem& sm, const TableView& tb, const RecordView& rc,
-                              int it0, int tau0, int n_grp, int n_active, int n_stages,
-                              int rowcap, int* status, int lane, int& issued) {
-    (void)tb;
-    const unsigned char* tr = reinterpret_cast<const unsigned char*>(rc.traces);
-    const int row_words = rowcap * RF;
-    while (true) {
-      // lane 0 decides for the warp (the lanes stay converged)
-      const int go = (issued < n_stages && !*sm.abort_flag) ? 1 : 0;
-      if (!__shfl_sync(0xFFFFFFFFu, go, 0)) break;
-      const int it = it0 + issued;
-      const int stage = it % NSTAGE;
-      if (it >= NSTAGE) {
-        // every lane observes the slot's release itself (acquire) before any
-        // lane's copy may overwrite it
-        const bool free_slot = mbar_try_wait(&sm.empty[stage], ((it / NSTAGE) - 1) & 1);
-        if (!__all_sync(0xFFFFFFFFu, free_slot)) break;
-      }
-      const int r = issued;
-      const int tau = tau0 + r / n_grp;
-      const int j0 = (r - (r / n_grp) * n_grp) * SPS;
-      const int nj = min(SPS, n_active - j0);
-      const int t0 = tau * TT;
-      auto copy_ok = [&](int j, int p) -> bool {
-#if BP_DEBUG_CHECKS
-        const int s = sm.st_s[j];
-        const int w = min(sm.st_w[j * P + p], rowcap);
-        const long long col = (long long)rc.lpad + t0 + sm.st_lo[j * P + p];
-        return s >= 0 && s < tb.S && w > 0 && col >= 0 && col + w <= rc.pitch &&
-               (col * ESZ) % 16 == 0 && ((long long)w * ESZ) % 16 == 0;
-#else
-        (void)j;
-        (void)p;
-        return true;
-#endif
-      };
-      if (lane == 0) {
-        uint32_t bytes = 0;
-#pragma unroll
-        for (int jj = 0; jj < SPS; ++jj) {
-          if (jj >= nj) break;
-#pragma unroll
-          for (int p = 0; p < P; ++p)
-            if (copy_ok(j0 + jj, p))
-              bytes += (uint32_t)min(sm.st_w[(j0 + jj) * P + p], rowcap) * ESZ * NVER;
-            else
-              atomicOr(status, kStatusBadIndex);
-        }
-        mbar_arrive_expect_tx(&sm.full[stage], bytes);
-      }
-      __syncwarp();
-      for (int c = lane; c < nj * P * NVER; c += 32) {
-        const int jj = c / (P * NVER);
-        const int p = (c / NVER) % P;
-        const int v = c % NVER;
-        const int j = j0 + jj;
-        if (!copy_ok(j, p)) continue;
-        const int s = sm.st_s[j];
-        const int w = min(sm.st_w[j * P + p], rowcap);
-        const long long col = (long long)rc.lpad + t0 + sm.st_lo[j * P + p];
-        const size_t row = (size_t)(s * P + p) * NVER + v;
-        bulk_g2s(sm.ring + ((size_t)((stage * SPS + jj) * P + p) * row_words) * 4 +
-                     (size_t)v * rowcap * ESZ,
-                 tr + (row * rc.pitch + col) * ESZ, (uint32_t)w * ESZ, &sm.full[stage]);
-      }
-      __syncwarp();
-      ++issued;
-    }
   }
 
   // The consumer warps' part of an item: for every time tile, the stages'
   // stations into the accumulators, then the epilogue.  FAST16: the item's
   // weight words hold packed 16-bit factors (block-uniform choice).
   template <bool FAST16>
-  __device__ static void consume(const Smem& sm, const TableView& tb, const RecordView& rc,
-                                 int tau0, int tau1, int n_active, int n_grp, int rowcap,
-                                 int* status, int it0) {
+  __device__ static void consume(const Smem& sm, const RecordView& rc, int tau0, int tau1,
+                                 int n_active, int n_grp, int rowcap, int* status, int it0) {
     const int tid = threadIdx.x;
     const int warp = tid >> 5;
     const int lane = tid & 31;
     const int row_words = rowcap * RF;
     const int4* my_src = sm.srci + warp * KS;
     int it = it0;
-    // INL: stages issued so far by warp 0 (relative to it0)
-    const int n_stages = (tau1 - tau0) * n_grp;
-    int issued = 0;
-    (void)tb;
-    (void)n_stages;
-    (void)issued;
     for (int tau = tau0; tau < tau1; ++tau) {
       float2 acc[KS][MT / 2];  // pair q, half h: sample pair_sample(lane, q, h)
 #pragma unroll
@@ -809,39 +724,7 @@ struct Staged {
 
       for (int g = 0; g < n_grp; ++g, ++it) {
         const int stage = it % NSTAGE;
-        if constexpr (INL) {
-          if (warp == 0) {
-            // refill what the other warps have released, then wait for this
-            // stage, refilling while it is in flight (bounded like every wait)
-            pump(sm, tb, rc, it0, tau0, n_grp, n_active, n_stages, rowcap, status, lane, issued);
-            // every lane observes the stage's completion itself (acquire);
-            // lane 0 alone decides to give up, so the lanes stay converged
-            if (!__all_sync(0xFFFFFFFFu, mbar_try_wait(&sm.full[stage], (it / NSTAGE) & 1))) {
-              const unsigned long long start = globaltimer_ns();
-              while (true) {
-                pump(sm, tb, rc, it0, tau0, n_grp, n_active, n_stages, rowcap, status, lane,
-                     issued);
-                const bool landed = mbar_try_wait(&sm.full[stage], (it / NSTAGE) & 1);
-                if (__all_sync(0xFFFFFFFFu, landed)) break;
-                int stop = 0;
-                if (lane == 0) {
-                  if (*sm.abort_flag) {
-                    stop = 1;
-                  } else if (globaltimer_ns() - start > kWaitLimitNs) {
-                    *sm.abort_flag = 1;
-                    atomicOr(status, kStatusWaitTimeout);
-                    stop = 1;
-                  }
-                }
-                if (__shfl_sync(0xFFFFFFFFu, stop, 0)) break;
-              }
-            }
-          } else {
-            mbar_wait_bounded(&sm.full[stage], (it / NSTAGE) & 1, sm.abort_flag, status);
-          }
-        } else {
-          mbar_wait_bounded(&sm.full[stage], (it / NSTAGE) & 1, sm.abort_flag, status);
-        }
+        mbar_wait_bounded(&sm.full[stage], (it / NSTAGE) & 1, sm.abort_flag, status);
 #pragma unroll
         for (int jj = 0; jj < SPS; ++jj) {
           const int j = g * SPS + jj;
@@ -947,16 +830,6 @@ struct Staged {
               if (t >= si.y && t < si.z) row[t] = h ? acc[k][q].y : acc[k][q].x;
             }
           }
-        }
-      }
-    }
-    if constexpr (INL) {
-      if (warp == 0 && *sm.abort_flag) {
-        // Let every copy already issued land before the block moves on.
-        volatile int never = 0;
-        for (int r = max(0, issued - NSTAGE); r < issued; ++r) {
-          const int itr = it0 + r;
-          mbar_wait_bounded(&sm.full[itr % NSTAGE], (itr / NSTAGE) & 1, &never, nullptr);
         }
       }
     }
@@ -1184,10 +1057,10 @@ struct Staged {
 // time-chunk major so that the blocks in flight share an L2-resident stretch
 // of trace.
 template <int P, int KS, int MT, int WS, int NSTAGE, int SPS, int MINB, bool MAXRED,
-          bool CHECKED, int STORAGE, bool INL>
-__global__ void __launch_bounds__((WS + (INL ? 0 : 1)) * 32, MINB)
+          bool CHECKED, int STORAGE>
+__global__ void __launch_bounds__((WS + 1) * 32, MINB)
 beam_window_kernel(const LaunchArgs a) {
-  using St = Staged<P, KS, MT, WS, NSTAGE, SPS, MAXRED, CHECKED, STORAGE, INL>;
+  using St = Staged<P, KS, MT, WS, NSTAGE, SPS, MAXRED, CHECKED, STORAGE>;
   extern __shared__ __align__(128) unsigned char smem[];
   const typename St::Smem sm = St::carve(smem, a.rowcap, a.max_active, a.red_rows);
   if (threadIdx.x == 0) St::init_barriers(sm);
@@ -1209,10 +1082,10 @@ beam_window_kernel(const LaunchArgs a) {
 // differ in length, station subset and table; storage, phases and reduce are
 // the launch's.
 template <int P, int KS, int MT, int WS, int NSTAGE, int SPS, int MINB, bool MAXRED,
-          bool CHECKED, int STORAGE, bool INL>
-__global__ void __launch_bounds__((WS + (INL ? 0 : 1)) * 32, MINB)
+          bool CHECKED, int STORAGE>
+__global__ void __launch_bounds__((WS + 1) * 32, MINB)
 beam_batch_kernel(const LaunchArgs a) {
-  using St = Staged<P, KS, MT, WS, NSTAGE, SPS, MAXRED, CHECKED, STORAGE, INL>;
+  using St = Staged<P, KS, MT, WS, NSTAGE, SPS, MAXRED, CHECKED, STORAGE>;
   extern __shared__ __align__(128) unsigned char smem[];
   const typename St::Smem sm = St::carve(smem, a.rowcap, a.max_active, a.red_rows);
   if (threadIdx.x == 0) St::init_barriers(sm);

@@ -21,10 +21,10 @@ int launch_window_p(const bp::LaunchArgs& a, bool batch, long long plain_blocks,
   if (STORAGE != BP_STORAGE_F32 && (long long)a.rowcap * 8 >= 65536)
     return fail(BP_ERR_UNSUPPORTED, "16-bit storage: ring rows of %d samples are too long",
                 a.rowcap);
-  constexpr int threads = C::THREADS;
+  constexpr int threads = bp::WindowCfg<P, C::KS, C::MT, C::WS>::kThreads;
   if (batch) {
     auto kern = bp::beam_batch_kernel<P, C::KS, C::MT, C::WS, C::NSTAGE, C::SPS, C::MINB,
-                                      MAXRED, CHECKED, STORAGE, C::INL>;
+                                      MAXRED, CHECKED, STORAGE>;
     BP_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)lay.total));
     int per_sm = 0;
@@ -34,7 +34,7 @@ int launch_window_p(const bp::LaunchArgs& a, bool batch, long long plain_blocks,
     BP_LAUNCHED("beam_batch_kernel");
   } else {
     auto kern = bp::beam_window_kernel<P, C::KS, C::MT, C::WS, C::NSTAGE, C::SPS, C::MINB,
-                                       MAXRED, CHECKED, STORAGE, C::INL>;
+                                       MAXRED, CHECKED, STORAGE>;
     BP_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)lay.total));
     if (plain_blocks > kMaxInt) return fail(BP_ERR_UNSUPPORTED, "grid too large");
