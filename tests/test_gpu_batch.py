@@ -43,14 +43,21 @@ def _expected(oracle_lib, A, grids, w, F):
     return oracle_lib.beamform_max(U, D, W, 0 if w.out_of_bounds == "strict" else 1)
 
 
-def test_batch_matches_single_windows(cuda, oracle_lib):
+@pytest.mark.parametrize("cfg", [-1, 0, 2, 3, 8])
+def test_batch_matches_single_windows(cuda, oracle_lib, bplib, cfg):
+    """Every window equals the oracle on that window alone, bit for bit, in
+    the persistent kernel of the default shape and of shapes forced here."""
     import torch
     from beampower_b200.batch import WindowBatch
     from beampower_b200.tables import TravelTimeTable
     rng, A, grids = _network(1)
     tables = [TravelTimeTable(D, W) for D, W in grids]
     windows = _windows(rng, A.shape[0])
-    batch = WindowBatch(tables, windows, A, storage="fp32")
+    bplib.bp_set_kernel_config(0, 1, cfg)
+    try:
+        batch = WindowBatch(tables, windows, A, storage="fp32")
+    finally:
+        bplib.bp_set_kernel_config(0, 1, -1)
     feats = []
     for i, w in enumerate(windows):
         F = np.abs(rng.standard_normal((A.shape[0], A.shape[1], w.n_samples))).astype(np.float32)
