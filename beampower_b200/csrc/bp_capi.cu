@@ -459,7 +459,7 @@ int run_staged(const bp_table* t, const void* traces, int storage, const float* 
 int run_direct(const void* traces, int storage, const float* scales, size_t T, size_t lpad,
                size_t pitch, const int32_t* delays, const float* weights, const int32_t* minmax,
                size_t N, size_t S, size_t P, int out_of_bounds, unsigned long long* keys,
-               float* beam, size_t ldb, cudaStream_t st) {
+               float* beam, size_t ldb, cudaStream_t st, int index_base = 0) {
   if (T == 0 || N == 0) return BP_OK;
   bp::DirectArgs a{};
   a.traces = traces;
@@ -475,6 +475,7 @@ int run_direct(const void* traces, int storage, const float* scales, size_t T, s
   a.delays = delays;
   a.weights = weights;
   a.minmax = minmax;
+  a.index_base = index_base;
   a.keys = keys;
   a.beam = beam;
   a.ldb = (long long)ldb;
@@ -517,6 +518,22 @@ cudaStream_t host_stream() {
     cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
     dev_of_s = dev;
     retain_pool(dev);
+  }
+  return s;
+}
+
+// Per-thread second stream of the host entry points: host-buffer uploads
+// (a copy from pageable memory waits for the work already on its own stream,
+// so it is kept off the stream that runs the kernels) and the tables built
+// from them.
+cudaStream_t upload_stream() {
+  thread_local cudaStream_t s = nullptr;
+  thread_local int dev_of_s = -1;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (!s || dev_of_s != dev) {
+    cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+    dev_of_s = dev;
   }
   return s;
 }
@@ -579,9 +596,12 @@ uint64_t bp_launch_count(void) { return g_launches.load(); }
 // ---------------------------------------------------------------------------
 // Tables
 // ---------------------------------------------------------------------------
-int bp_table_create(const int32_t* d_delays, const float* d_weights, size_t N, size_t S,
-                    size_t P, void* stream, bp_table** out) {
-  BP_NVTX("bp_table_create");
+// A table whose source indexes start at `index_base` (a table over a block
+// of a larger grid's sources, whose keys are then global: the host path's
+// source chunks); bp_table_create is the case index_base = 0.
+static int table_create_based(const int32_t* d_delays, const float* d_weights, size_t N,
+                              size_t S, size_t P, void* stream, int index_base,
+                              bp_table** out) {
   g_last_error.clear();
   if (!out) return fail(BP_ERR_INVALID_ARGUMENT, "out_table is NULL");
   *out = nullptr;
@@ -628,6 +648,7 @@ int bp_table_create(const int32_t* d_delays, const float* d_weights, size_t N, s
   t->dev.S = (int)S;
   t->dev.P = (int)P;
   t->dev.K = K;
+  t->dev.index_base = index_base;
   t->dev.n_tiles = (int)n_tiles;
   t->dev.stats = reinterpret_cast<int*>(base + o_stats);
   t->status = reinterpret_cast<int*>(base + o_status);
@@ -716,6 +737,12 @@ int bp_table_create(const int32_t* d_delays, const float* d_weights, size_t N, s
   }
   *out = t;
   return BP_OK;
+}
+
+int bp_table_create(const int32_t* d_delays, const float* d_weights, size_t N, size_t S,
+                    size_t P, void* stream, bp_table** out) {
+  BP_NVTX("bp_table_create");
+  return table_create_based(d_delays, d_weights, N, S, P, stream, 0, out);
 }
 
 int bp_table_destroy(bp_table* t) {
@@ -823,6 +850,19 @@ int bp_traces_from_prestacked_dev(const float* U, size_t T, size_t S, size_t P, 
   return BP_OK;
 }
 
+// Max-reduces the keys of every (source, sample) of table `t` into `keys`
+// (not cleared here), with the table's source index base.
+static int max_keys(const bp_table* t, const void* traces, int storage, const float* scales,
+                    size_t T, size_t lpad, size_t pitch, int out_of_bounds,
+                    unsigned long long* keys, cudaStream_t st) {
+  if (t->info.uses_window_kernel)
+    return run_staged(t, traces, storage, scales, T, lpad, pitch, out_of_bounds, keys, nullptr,
+                      0, st);
+  return run_direct(traces, storage, scales, T, lpad, pitch, t->delays, t->weights, t->minmax,
+                    t->info.n_sources, t->info.n_stations, t->info.n_phases, out_of_bounds,
+                    keys, nullptr, 0, st, t->dev.index_base);
+}
+
 int bp_beamform_max_dev(const bp_table* t, const void* traces, int storage, const float* scales,
                         size_t T, size_t lpad, size_t pitch, int out_of_bounds,
                         unsigned long long* keys, float* beam_max, int32_t* argmax,
@@ -841,16 +881,8 @@ int bp_beamform_max_dev(const bp_table* t, const void* traces, int storage, cons
   if (int rc = check_layout(t, T, lpad, pitch)) return rc;
   cudaStream_t st = as_stream(stream);
   BP_CUDA(cudaMemsetAsync(keys, 0, T * sizeof(unsigned long long), st));
-  int rc;
-  if (t->info.uses_window_kernel) {
-    rc = run_staged(t, traces, storage, scales, T, lpad, pitch, out_of_bounds, keys, nullptr, 0,
-                    st);
-  } else {
-    rc = run_direct(traces, storage, scales, T, lpad, pitch, t->delays, t->weights, t->minmax,
-                    t->info.n_sources, t->info.n_stations, t->info.n_phases, out_of_bounds, keys,
-                    nullptr, 0, st);
-  }
-  if (rc) return rc;
+  if (int rc = max_keys(t, traces, storage, scales, T, lpad, pitch, out_of_bounds, keys, st))
+    return rc;
   bp::decode_keys_kernel<<<(unsigned)((T + 255) / 256), 256, 0, st>>>(keys, (int)T, beam_max,
                                                                       argmax);
   BP_LAUNCHED("decode_keys_kernel");
@@ -966,6 +998,92 @@ int host_path(cudaStream_t st, DevBufs& bufs, const int32_t* d_delays, const flo
   return BP_OK;
 }
 
+// Sources per chunk of the host path's pipeline (at least), and chunks at most.
+constexpr size_t kChunkMinSources = 65536;
+constexpr size_t kMaxChunks = 8;
+
+// reduce='max' from host buffers for many sources, as a pipeline: the sources
+// in up to kMaxChunks contiguous chunks; each chunk's delays and weights are
+// uploaded, and its table built, on the upload stream while the previous
+// chunk's kernel runs; the chunk tables' source indexes start at the chunk's
+// first source, and every chunk max-reduces into the same keys, so the result
+// is the single table's, bit for bit (the keys' max does not depend on the
+// order).  The features are prestacked per chunk (each table has its own
+// trace layout; the prestack is a fraction of a millisecond).
+int host_max_chunked(const float* F, const float* alpha, const int32_t* delays, const float* w,
+                     size_t T, size_t N, size_t S, size_t C, size_t P, int oob, int storage,
+                     float* beam_max, int32_t* argmax) {
+  cudaStream_t st = host_stream();
+  cudaStream_t up = upload_stream();
+  DevBufs bufs(st);
+  const size_t n_chunks = std::min(kMaxChunks, N / kChunkMinSources);
+  size_t chunk = (N + n_chunks - 1) / n_chunks;
+  chunk = (chunk + kTileSources - 1) / kTileSources * kTileSources;
+  float *d_F = nullptr, *d_a = nullptr, *d_w = nullptr;
+  int32_t* d_d = nullptr;
+  unsigned long long* d_keys = nullptr;
+  BP_CUDA(bufs.alloc(&d_d, N * S * P * sizeof(int32_t)));
+  BP_CUDA(bufs.alloc(&d_w, N * S * sizeof(float)));
+  BP_CUDA(bufs.alloc(&d_F, S * C * T * sizeof(float)));
+  BP_CUDA(bufs.alloc(&d_a, S * C * P * sizeof(float)));
+  BP_CUDA(bufs.alloc(&d_keys, T * sizeof(unsigned long long)));
+  BP_CUDA(cudaMemsetAsync(d_keys, 0, T * sizeof(unsigned long long), st));
+  // the allocations above are ordered on `st`; the upload stream waits for them
+  std::vector<cudaEvent_t> ev(n_chunks + 1, nullptr);
+  struct Cleanup {
+    std::vector<cudaEvent_t>& ev;
+    std::vector<bp_table*> tables;
+    cudaStream_t st;
+    ~Cleanup() {
+      cudaStreamSynchronize(st);
+      for (bp_table* t : tables) bp_table_destroy(t);
+      for (cudaEvent_t e : ev)
+        if (e) cudaEventDestroy(e);
+    }
+  } cleanup{ev, {}, st};
+  for (auto& e : ev) BP_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  BP_CUDA(cudaEventRecord(ev[n_chunks], st));
+  BP_CUDA(cudaStreamWaitEvent(up, ev[n_chunks], 0));
+  BP_CUDA(cudaMemcpyAsync(d_F, F, S * C * T * sizeof(float), cudaMemcpyHostToDevice, up));
+  BP_CUDA(cudaMemcpyAsync(d_a, alpha, S * C * P * sizeof(float), cudaMemcpyHostToDevice, up));
+  for (size_t k = 0; k < n_chunks; ++k) {
+    const size_t lo = k * chunk, n = std::min(N, lo + chunk) - lo;
+    if (lo >= N) break;
+    // upload and table of chunk k (overlapping the kernel of chunk k - 1)
+    BP_CUDA(cudaMemcpyAsync(d_d + lo * S * P, delays + lo * S * P, n * S * P * sizeof(int32_t),
+                            cudaMemcpyHostToDevice, up));
+    BP_CUDA(cudaMemcpyAsync(d_w + lo * S, w + lo * S, n * S * sizeof(float),
+                            cudaMemcpyHostToDevice, up));
+    bp_table* t = nullptr;
+    if (int rc = table_create_based(d_d + lo * S * P, d_w + lo * S, n, S, P, up, (int)lo, &t))
+      return rc;
+    cleanup.tables.push_back(t);
+    BP_CUDA(cudaEventRecord(ev[k], up));
+    // prestack and kernel of chunk k, after its upload and table
+    BP_CUDA(cudaStreamWaitEvent(st, ev[k], 0));
+    size_t lpad = 0, pitch = 0;
+    if (int rc = bp_trace_layout(t, T, &lpad, &pitch)) return rc;
+    void* d_traces = nullptr;
+    float* d_scales = nullptr;
+    BP_CUDA(bufs.alloc(&d_traces,
+                       S * P * pitch * (storage == BP_STORAGE_F32 ? 4 : 2 * bp::kHalfCopies)));
+    BP_CUDA(bufs.alloc(&d_scales, S * sizeof(float)));
+    if (int rc = bp_prestack_dev(d_F, d_a, T, S, C, P, storage, lpad, pitch, d_traces, d_scales,
+                                 st))
+      return rc;
+    if (int rc = max_keys(t, d_traces, storage, d_scales, T, lpad, pitch, oob, d_keys, st))
+      return rc;
+  }
+  std::vector<unsigned long long> keys(T);
+  BP_CUDA(cudaMemcpyAsync(keys.data(), d_keys, T * sizeof(unsigned long long),
+                          cudaMemcpyDeviceToHost, st));
+  BP_CUDA(cudaStreamSynchronize(st));
+  for (bp_table* t : cleanup.tables)
+    if (int rc = read_status(t, st)) return rc;
+  decode_keys_host(keys, beam_max, argmax);
+  return BP_OK;
+}
+
 int prestacked_entry(const float* U, const int* delays, const float* w, size_t T, size_t N,
                      size_t S, size_t P, int oob, int reduce, float* beam_max, int32_t* argmax,
                      float* beam) {
@@ -1076,6 +1194,8 @@ int bp_beamform_host(const float* F, const float* alpha, const int32_t* delays, 
     if (reduce == BP_REDUCE_MAX) std::fill(argmax, argmax + T, 0);
     return BP_OK;
   }
+  if (reduce == BP_REDUCE_MAX && N >= 2 * kChunkMinSources)
+    return host_max_chunked(F, alpha, delays, w, T, N, S, C, P, oob, storage, beam_max, argmax);
   cudaStream_t st = host_stream();
   DevBufs bufs(st);
   float *d_F = nullptr, *d_a = nullptr, *d_w = nullptr;

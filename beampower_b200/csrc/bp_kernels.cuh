@@ -63,6 +63,7 @@ struct TableDev {
   void* meta;        // [n_tiles * S * K] MetaT<P>
   int* stats;        // [kStatCount]
   const int* perm;   // optional [n_tiles * K] source order (nullptr: identity)
+  int index_base;    // added to every source index (a table over part of a grid)
 };
 
 enum : int {
@@ -137,7 +138,7 @@ __global__ void table_build_kernel(const int32_t* __restrict__ delays,
         }
       }
     }
-    tb.src_info[(size_t)tile * K + k] = make_int4(o, mn, mx, 0);
+    tb.src_info[(size_t)tile * K + k] = make_int4(o >= 0 ? o + tb.index_base : o, mn, mx, 0);
     if (bad) atomicOr(&tb.stats[kStatNonFinite], 1);
   }
   // 2. per (station, phase): window over the tile's weighted sources.
@@ -1205,6 +1206,7 @@ struct DirectArgs {
   const int32_t* delays;
   const float* weights;
   const int32_t* minmax;   // (N, 2)
+  int index_base;          // added to the source index of every key
   unsigned long long* keys;
   float* beam;
   long long ldb;
@@ -1240,7 +1242,7 @@ __global__ void __launch_bounds__(256) beam_direct_kernel(const DirectArgs a) {
     }
     if constexpr (MAXRED) {
       if (valid) {
-        const unsigned long long key = make_key(acc, i);
+        const unsigned long long key = make_key(acc, i + a.index_base);
         best = key > best ? key : best;
       }
     } else {
