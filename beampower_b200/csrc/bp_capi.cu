@@ -525,14 +525,17 @@ cudaStream_t host_stream() {
 // Per-thread second stream of the host entry points: host-buffer uploads
 // (a copy from pageable memory waits for the work already on its own stream,
 // so it is kept off the stream that runs the kernels) and the tables built
-// from them.
+// from them.  Highest priority: a table build's short kernels take SMs ahead
+// of the long kernel running beside them on the other stream.
 cudaStream_t upload_stream() {
   thread_local cudaStream_t s = nullptr;
   thread_local int dev_of_s = -1;
   int dev = 0;
   cudaGetDevice(&dev);
   if (!s || dev_of_s != dev) {
-    cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+    int least = 0, greatest = 0;
+    cudaDeviceGetStreamPriorityRange(&least, &greatest);
+    cudaStreamCreateWithPriority(&s, cudaStreamNonBlocking, greatest);
     dev_of_s = dev;
   }
   return s;
