@@ -1042,7 +1042,6 @@ def run_shapes(args, local_rank):
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
     lib = load_library("gpu")
-    os.environ.setdefault(autotune.CACHE_ENV, os.path.join("/tmp", "bp_shapes_cache.json"))
     wl = make_workload(LARGE)
     bw = make_batch_workload(n_windows=1)
     D50, W50 = bw["grids"][1]
