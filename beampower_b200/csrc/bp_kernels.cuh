@@ -619,34 +619,43 @@ struct Staged {
     const int n_stages = (tau1 - tau0) * n_grp;
 
     // ---- producer warp ----------------------------------------------------
+    // Lane 0 waits for the stage to drain and arms its full barrier with the
+    // stage's byte count; the warp's lanes then issue the stage's copies
+    // (stations x phases x row copies, up to 16 with 16-bit storage) side by
+    // side, so the issue of one stage is no longer a serial chain of one lane.
     if (warp == WS) {
-      if (lane == 0) {
-        const unsigned char* tr = reinterpret_cast<const unsigned char*>(rc.traces);
-        int issued = 0;
-        for (int r = 0; r < n_stages; ++r) {
-          const int it = it0 + r;
-          const int stage = it % NSTAGE;
-          if (it >= NSTAGE && !mbar_wait_bounded(&sm.empty[stage], ((it / NSTAGE) - 1) & 1,
-                                                 sm.abort_flag, status))
-            break;
-          const int tau = tau0 + r / n_grp;
-          const int j0 = (r - (r / n_grp) * n_grp) * SPS;
-          const int nj = min(SPS, n_active - j0);
-          const int t0 = tau * TT;
-          // copy (jj, p, v) reads trace row (s P + p) NVER + v, columns [col, col + w)
-          auto copy_ok = [&](int j, int p) -> bool {
+      const unsigned char* tr = reinterpret_cast<const unsigned char*>(rc.traces);
+      int issued = 0;
+      for (int r = 0; r < n_stages; ++r) {
+        const int it = it0 + r;
+        const int stage = it % NSTAGE;
+        int ok = 1;
+        if (lane == 0 && it >= NSTAGE)
+          ok = mbar_wait_bounded(&sm.empty[stage], ((it / NSTAGE) - 1) & 1, sm.abort_flag,
+                                 status) ? 1 : 0;
+        if (!__shfl_sync(0xFFFFFFFFu, ok, 0)) break;
+        // every issuing lane observes the drained phase itself before its
+        // copies overwrite the stage (the phase has completed: no wait)
+        if (it >= NSTAGE) (void)mbar_try_wait(&sm.empty[stage], ((it / NSTAGE) - 1) & 1);
+        const int tau = tau0 + r / n_grp;
+        const int j0 = (r - (r / n_grp) * n_grp) * SPS;
+        const int nj = min(SPS, n_active - j0);
+        const int t0 = tau * TT;
+        // copy (jj, p, v) reads trace row (s P + p) NVER + v, columns [col, col + w)
+        auto copy_ok = [&](int j, int p) -> bool {
 #if BP_DEBUG_CHECKS
-            const int s = sm.st_s[j];
-            const int w = min(sm.st_w[j * P + p], rowcap);
-            const long long col = (long long)rc.lpad + t0 + sm.st_lo[j * P + p];
-            return s >= 0 && s < tb.S && w > 0 && col >= 0 && col + w <= rc.pitch &&
-                   (col * ESZ) % 16 == 0 && ((long long)w * ESZ) % 16 == 0;
+          const int s = sm.st_s[j];
+          const int w = min(sm.st_w[j * P + p], rowcap);
+          const long long col = (long long)rc.lpad + t0 + sm.st_lo[j * P + p];
+          return s >= 0 && s < tb.S && w > 0 && col >= 0 && col + w <= rc.pitch &&
+                 (col * ESZ) % 16 == 0 && ((long long)w * ESZ) % 16 == 0;
 #else
-            (void)j;
-            (void)p;
-            return true;
+          (void)j;
+          (void)p;
+          return true;
 #endif
-          };
+        };
+        if (lane == 0) {
           uint32_t bytes = 0;
 #pragma unroll
           for (int jj = 0; jj < SPS; ++jj) {
@@ -659,35 +668,30 @@ struct Staged {
                 atomicOr(status, kStatusBadIndex);
           }
           mbar_arrive_expect_tx(&sm.full[stage], bytes);
-#pragma unroll
-          for (int jj = 0; jj < SPS; ++jj) {
-            if (jj >= nj) break;
-            const int j = j0 + jj;
-            const int s = sm.st_s[j];
-#pragma unroll
-            for (int p = 0; p < P; ++p) {
-              if (!copy_ok(j, p)) continue;
-              const int w = min(sm.st_w[j * P + p], rowcap);
-              const long long col = (long long)rc.lpad + t0 + sm.st_lo[j * P + p];
-              unsigned char* dst =
-                  sm.ring + ((size_t)((stage * SPS + jj) * P + p) * row_words) * 4;
-#pragma unroll
-              for (int v = 0; v < NVER; ++v) {
-                const size_t row = (size_t)(s * P + p) * NVER + v;
-                bulk_g2s(dst + (size_t)v * rowcap * ESZ, tr + (row * rc.pitch + col) * ESZ,
-                         (uint32_t)w * ESZ, &sm.full[stage]);
-              }
-            }
-          }
-          ++issued;
         }
-        if (*sm.abort_flag) {
-          // Let every copy already issued land before the block moves on.
-          volatile int never = 0;
-          for (int r = max(0, issued - NSTAGE); r < issued; ++r) {
-            const int it = it0 + r;
-            mbar_wait_bounded(&sm.full[it % NSTAGE], (it / NSTAGE) & 1, &never, nullptr);
-          }
+        __syncwarp();
+        for (int c = lane; c < nj * P * NVER; c += 32) {
+          const int jj = c / (P * NVER);
+          const int p = (c / NVER) % P;
+          const int v = c % NVER;
+          const int j = j0 + jj;
+          if (!copy_ok(j, p)) continue;
+          const int s = sm.st_s[j];
+          const int w = min(sm.st_w[j * P + p], rowcap);
+          const long long col = (long long)rc.lpad + t0 + sm.st_lo[j * P + p];
+          const size_t row = (size_t)(s * P + p) * NVER + v;
+          bulk_g2s(sm.ring + ((size_t)((stage * SPS + jj) * P + p) * row_words) * 4 +
+                       (size_t)v * rowcap * ESZ,
+                   tr + (row * rc.pitch + col) * ESZ, (uint32_t)w * ESZ, &sm.full[stage]);
+        }
+        ++issued;
+      }
+      if (lane == 0 && *sm.abort_flag) {
+        // Let every copy already issued land before the block moves on.
+        volatile int never = 0;
+        for (int r = max(0, issued - NSTAGE); r < issued; ++r) {
+          const int it = it0 + r;
+          mbar_wait_bounded(&sm.full[it % NSTAGE], (it / NSTAGE) & 1, &never, nullptr);
         }
       }
       return n_stages;
