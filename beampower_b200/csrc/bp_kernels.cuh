@@ -442,6 +442,14 @@ struct Staged {
   // 16-bit storage with at most 32 accumulators per thread: the words of both
   // sources of a metadata pair are loaded before either's arithmetic.
   static constexpr bool PAIRLOAD = !F32 && KS * MT <= 32 && MT == GS;
+  // Who issues one stage's bulk copies (SPS stations x P phases x NVER row
+  // copies): lane 0 alone, or one producer lane per (station, phase) row with
+  // its NVER copies.  Rows in parallel pay for 16-bit storage with two
+  // stations per stage (16 copies a stage at P = 2; 400k-source workload,
+  // config 2 FP16 488 -> 420 ms, config 5 506 -> 445 ms); with one station
+  // per stage, or FP32's P x SPS copies, lane 0 alone measured 1-7% faster.
+  static constexpr int kIssueLane0 = 0, kIssueRow = 1;
+  static constexpr int ISSUE = (!F32 && SPS > 1) ? kIssueRow : kIssueLane0;
 
   struct Smem {
     unsigned char* ring;
@@ -620,10 +628,9 @@ struct Staged {
 
     // ---- producer warp ----------------------------------------------------
     // Lane 0 waits for the stage to drain and arms its full barrier with the
-    // stage's byte count; the warp's lanes then issue the stage's copies
-    // (stations x phases x row copies, up to 16 with 16-bit storage) side by
-    // side, so the issue of one stage is no longer a serial chain of one lane.
+    // stage's byte count; the stage's copies are then issued as ISSUE says.
     if (warp == WS) {
+      if (ISSUE == kIssueLane0 && lane != 0) return n_stages;
       const unsigned char* tr = reinterpret_cast<const unsigned char*>(rc.traces);
       int issued = 0;
       for (int r = 0; r < n_stages; ++r) {
@@ -633,10 +640,14 @@ struct Staged {
         if (lane == 0 && it >= NSTAGE)
           ok = mbar_wait_bounded(&sm.empty[stage], ((it / NSTAGE) - 1) & 1, sm.abort_flag,
                                  status) ? 1 : 0;
-        if (!__shfl_sync(0xFFFFFFFFu, ok, 0)) break;
-        // every issuing lane observes the drained phase itself before its
-        // copies overwrite the stage (the phase has completed: no wait)
-        if (it >= NSTAGE) (void)mbar_try_wait(&sm.empty[stage], ((it / NSTAGE) - 1) & 1);
+        if constexpr (ISSUE != kIssueLane0) {
+          if (!__shfl_sync(0xFFFFFFFFu, ok, 0)) break;
+          // every issuing lane observes the drained phase itself before its
+          // copies overwrite the stage (the phase has completed: no wait)
+          if (it >= NSTAGE) (void)mbar_try_wait(&sm.empty[stage], ((it / NSTAGE) - 1) & 1);
+        } else {
+          if (!ok) break;
+        }
         const int tau = tau0 + r / n_grp;
         const int j0 = (r - (r / n_grp) * n_grp) * SPS;
         const int nj = min(SPS, n_active - j0);
@@ -669,20 +680,49 @@ struct Staged {
           }
           mbar_arrive_expect_tx(&sm.full[stage], bytes);
         }
-        __syncwarp();
-        for (int c = lane; c < nj * P * NVER; c += 32) {
-          const int jj = c / (P * NVER);
-          const int p = (c / NVER) % P;
-          const int v = c % NVER;
+        if constexpr (ISSUE != kIssueLane0) __syncwarp();
+        // Row (jj, p): station slot j0 + jj, phase p; its NVER copies go to
+        // consecutive ring rows.  The row's index, width and offset are read
+        // once: every bulk copy's memory clobber would reload them.
+        struct RowSpan {
+          unsigned char* dst;
+          const unsigned char* src;
+          uint32_t bytes;
+        };
+        auto row_span = [&](int jj, int p) -> RowSpan {
           const int j = j0 + jj;
-          if (!copy_ok(j, p)) continue;
           const int s = sm.st_s[j];
           const int w = min(sm.st_w[j * P + p], rowcap);
           const long long col = (long long)rc.lpad + t0 + sm.st_lo[j * P + p];
-          const size_t row = (size_t)(s * P + p) * NVER + v;
-          bulk_g2s(sm.ring + ((size_t)((stage * SPS + jj) * P + p) * row_words) * 4 +
-                       (size_t)v * rowcap * ESZ,
-                   tr + (row * rc.pitch + col) * ESZ, (uint32_t)w * ESZ, &sm.full[stage]);
+          const size_t row0 = (size_t)(s * P + p) * NVER;
+          return {sm.ring + ((size_t)((stage * SPS + jj) * P + p) * row_words) * 4,
+                  tr + (row0 * rc.pitch + col) * ESZ, (uint32_t)w * ESZ};
+        };
+        auto issue = [&](const RowSpan& r, int v) {
+          bulk_g2s(r.dst + (size_t)v * rowcap * ESZ, r.src + (size_t)v * rc.pitch * ESZ, r.bytes,
+                   &sm.full[stage]);
+        };
+        if constexpr (ISSUE == kIssueLane0) {
+#pragma unroll
+          for (int jj = 0; jj < SPS; ++jj) {
+            if (jj >= nj) break;
+#pragma unroll
+            for (int p = 0; p < P; ++p) {
+              if (!copy_ok(j0 + jj, p)) continue;
+              const RowSpan r = row_span(jj, p);
+#pragma unroll
+              for (int v = 0; v < NVER; ++v) issue(r, v);
+            }
+          }
+        } else {
+          for (int q = lane; q < nj * P; q += 32) {
+            const int jj = q / P;
+            const int p = q - jj * P;
+            if (!copy_ok(j0 + jj, p)) continue;
+            const RowSpan r = row_span(jj, p);
+#pragma unroll
+            for (int v = 0; v < NVER; ++v) issue(r, v);
+          }
         }
         ++issued;
       }
