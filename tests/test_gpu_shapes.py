@@ -77,7 +77,7 @@ def test_config_count_and_shapes(cuda, bplib):
     assert {8, 16, 32} <= mts and {2, 4, 8} <= kss and {1, 2} <= spss
 
 
-@pytest.mark.parametrize("P", [1, 2, 3])
+@pytest.mark.parametrize("P", [1, 2, 3, 4])
 def test_every_shape_fp32_matches_oracle(cuda, bplib, oracle_lib, P):
     from beampower_b200.tables import TravelTimeTable
     F, A, D, W = _network(10 + P, P=P, unit=False)
@@ -159,7 +159,7 @@ def _model_16bit(tr, D, W, storage, oob):
 
 
 @pytest.mark.parametrize("storage", ["fp16", "bf16"])
-@pytest.mark.parametrize("P", [1, 2, 3])
+@pytest.mark.parametrize("P", [1, 2, 3, 4])
 def test_16bit_unit_weights_exact_model(cuda, bplib, storage, P):
     from beampower_b200.core import STORAGE
     from beampower_b200.tables import TravelTimeTable
