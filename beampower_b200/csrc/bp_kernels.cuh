@@ -228,23 +228,24 @@ __global__ void table_build_kernel(const int32_t* __restrict__ delays,
 }
 
 // ---------------------------------------------------------------------------
-// Staged shift-and-stack kernel (FP32 storage).
+// Staged shift-and-stack kernel.
 //
 // Block = WS consumer warps + 1 producer warp, one source tile of
 // K = WS * KS sources, a contiguous chunk of time tiles of TT = 32 * MT
-// samples.  For every (time tile, active station) the producer's elected
-// lane copies the station's P delay windows, [t0 + lo, t0 + lo + W), from
-// HBM/L2 into a shared-memory ring of NSTAGE stages with 1-D bulk copies
-// (TMA engine, 16-byte aligned, completing on the stage's "full" mbarrier).
-// Consumer warp w owns sources w*KS .. w*KS+KS-1; lane l owns samples
+// samples.  For every (time tile, group of SPS active stations) the producer
+// copies the stations' P delay windows, [t0 + lo, t0 + lo + W), from HBM/L2
+// into a shared-memory ring of NSTAGE stages with 1-D bulk copies (TMA
+// engine, 16-byte aligned, completing on the stage's "full" mbarrier); 16-bit
+// storage copies each window four times, shifted by one sample.  Consumer
+// warp w owns sources w*KS .. w*KS+KS-1; with FP32 storage lane l owns samples
 // t0 + l + 32*m, m < MT, so each warp-wide shared load reads 32 consecutive
-// words (one conflict-free wavefront) and the per-(source, station) metadata
-// is a broadcast.  Accumulation: acc = acc + w * u, rounded multiply then
-// rounded add, stations ascending, phases ascending (reference order).
-// After the last station of a time tile: strict-validity mask, packed key
-// per (source, sample), max over the thread's sources, then over the WS
-// warps through shared memory, then one red.global.max.u64 per sample; or,
-// for reduce='none', coalesced stores of the tile's beams.
+// words (one conflict-free wavefront), and the per-(source, station) metadata
+// is a broadcast.  FP32 accumulation: acc = acc + w * u, rounded multiply
+// then rounded add, stations ascending, phases ascending (reference order).
+// After the last station of a time tile: per sample the thread's best
+// (value, source) over its KS sources, one packed key per sample, a max over
+// the WS warps through shared memory, then one red.global.max.u64 per sample;
+// or, for reduce='none', coalesced stores of the tile's beams.
 // ---------------------------------------------------------------------------
 // A travel-time table as the staged kernel reads it.
 struct TableView {
