@@ -1526,10 +1526,10 @@ __global__ void sort_tile_slots_kernel(int* __restrict__ perm, int N) {
 // ---------------------------------------------------------------------------
 // 16-bit trace storage (BF16 / FP16 with a per-station scale).
 //
-// Each (station, phase) row is stored twice: version 0 holds x[t] at index
-// lpad + t, version 1 holds x[t + 1] there.  Row (s * P + p) * 2 + v of
-// `pitch` 16-bit elements.  A pair of consecutive samples (x[a], x[a + 1]) is
-// then always one aligned 32-bit word: version a & 1, index lpad + a - (a & 1).
+// Each (station, phase) row is stored kHalfCopies = 4 times: version v holds
+// x[t + v] at index lpad + t.  Row (s * P + p) * 4 + v of `pitch` 16-bit
+// elements.  A run of four consecutive samples x[a .. a + 3] is then always
+// one aligned 64-bit word: version a & 3, index lpad + a - (a & 3).
 // The stored value is U / scale_s with scale_s a power of two >= max |U| of
 // the station (1 for an all-zero station), so the scaling itself is exact and
 // only the rounding to 16 bits loses precision.
