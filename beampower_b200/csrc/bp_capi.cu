@@ -384,6 +384,15 @@ int config_for(const bp_table* t, int storage, bool maxred) {
   return 0;
 }
 
+// Whether some staged shape serves table `t` with this storage and reduction
+// (tables too wide for every shape's ring run the direct kernel).
+bool staged_serves(const bp_table* t, int storage, bool maxred) {
+  if (!t->info.uses_window_kernel) return false;
+  for (int c = 0; c < kNumConfigs; ++c)
+    if (config_fits(t, c, storage, maxred)) return true;
+  return false;
+}
+
 int choose_tiles_per_chunk(int n_tt, int n_tiles, int dev) {
   // Enough blocks for load balance (>= ~16 per SM), chunks of at most 64 time
   // tiles so that the blocks in flight share an L2-resident stretch of trace.
@@ -713,16 +722,13 @@ static int table_create_based(const int32_t* d_delays, const float* d_weights, s
   in.max_spread = stats[bp::kStatMaxSpread];
   in.max_active = stats[bp::kStatMaxActive];
   in.any_nonfinite = stats[bp::kStatNonFinite];
-  bool use_window = window && n_tiles > 0 && !stats[bp::kStatWideTile];
-  if (use_window) {
-    const int rowcap = (int)bp::align_up_sz((size_t)(cfg_time_tile(0) + in.max_spread + 1),
-                                            bp::kAlign);
-    // sized for the largest storage, so that the choice holds for every call
-    const size_t need =
-        staged_smem_bytes(0, (int)P, true, rowcap, std::max(1, in.max_active), -1, 1);
-    if (need > (size_t)device_smem_optin(t->device)) use_window = false;
-  }
-  in.uses_window_kernel = use_window ? 1 : 0;
+  // The staged kernel serves the table when some shape holds its windows
+  // with FP32 storage (the smallest ring).  16-bit storage keeps four copies
+  // of every window and may fit no shape where FP32 does; such calls expand
+  // their traces to FP32 and run the FP32 shapes (run_staged_expanded).
+  in.uses_window_kernel = window && n_tiles > 0 && !stats[bp::kStatWideTile] ? 1 : 0;
+  if (in.uses_window_kernel && !staged_serves(t, BP_STORAGE_F32, true)) in.uses_window_kernel = 0;
+  const bool use_window = in.uses_window_kernel != 0;
   if (!use_window && N > 0) {
     // The direct kernel reads the raw arrays: keep private copies.
     e = cudaMallocAsync(&t->direct_mem, N * S * P * sizeof(int32_t) + N * S * sizeof(float) + 256,
@@ -853,14 +859,47 @@ int bp_traces_from_prestacked_dev(const float* U, size_t T, size_t S, size_t P, 
   return BP_OK;
 }
 
+// 16-bit traces of a table whose four-copy windows fit no staged shape while
+// its FP32 windows do: the rows are expanded to FP32 in a scratch buffer
+// (value * scale_s, exact) and the FP32 staged kernel runs on them.  Per term
+// it forms round(w * (u * scale_s)) and adds it with one rounding, stations
+// then phases ascending: the value and order of the direct kernel's 16-bit
+// path, at the staged kernel's speed.
+static int run_staged_expanded(const bp_table* t, const void* traces, int storage,
+                               const float* scales, size_t T, size_t lpad, size_t pitch,
+                               int out_of_bounds, unsigned long long* keys, float* beam,
+                               size_t ldb, cudaStream_t st) {
+  const int S = t->dev.S, P = t->dev.P;
+  float* f32 = nullptr;
+  BP_CUDA(cudaMallocAsync(&f32, (size_t)S * P * pitch * sizeof(float), st));
+  struct Scratch32 {
+    float* p;
+    cudaStream_t s;
+    ~Scratch32() { cudaFreeAsync(p, s); }
+  } guard{f32, st};
+  const dim3 grid((unsigned)((pitch + 255) / 256), (unsigned)(S * P));
+  if (storage == BP_STORAGE_BF16)
+    bp::expand_h16_kernel<BP_STORAGE_BF16><<<grid, 256, 0, st>>>(traces, scales, P,
+                                                                 (long long)pitch, f32);
+  else
+    bp::expand_h16_kernel<BP_STORAGE_F16><<<grid, 256, 0, st>>>(traces, scales, P,
+                                                                (long long)pitch, f32);
+  BP_LAUNCHED("expand_h16_kernel");
+  return run_staged(t, f32, BP_STORAGE_F32, nullptr, T, lpad, pitch, out_of_bounds, keys, beam,
+                    ldb, st);
+}
+
 // Max-reduces the keys of every (source, sample) of table `t` into `keys`
 // (not cleared here), with the table's source index base.
 static int max_keys(const bp_table* t, const void* traces, int storage, const float* scales,
                     size_t T, size_t lpad, size_t pitch, int out_of_bounds,
                     unsigned long long* keys, cudaStream_t st) {
-  if (t->info.uses_window_kernel)
+  if (staged_serves(t, storage, true))
     return run_staged(t, traces, storage, scales, T, lpad, pitch, out_of_bounds, keys, nullptr,
                       0, st);
+  if (storage != BP_STORAGE_F32 && staged_serves(t, BP_STORAGE_F32, true))
+    return run_staged_expanded(t, traces, storage, scales, T, lpad, pitch, out_of_bounds, keys,
+                               nullptr, 0, st);
   return run_direct(traces, storage, scales, T, lpad, pitch, t->delays, t->weights, t->minmax,
                     t->info.n_sources, t->info.n_stations, t->info.n_phases, out_of_bounds,
                     keys, nullptr, 0, st, t->dev.index_base);
@@ -907,9 +946,12 @@ int bp_beamform_dev(const bp_table* t, const void* traces, int storage, const fl
   if (storage != BP_STORAGE_F32 && !scales)
     return fail(BP_ERR_INVALID_ARGUMENT, "16-bit storage needs scales");
   if (int rc = check_layout(t, T, lpad, pitch)) return rc;
-  if (t->info.uses_window_kernel)
+  if (staged_serves(t, storage, false))
     return run_staged(t, traces, storage, scales, T, lpad, pitch, out_of_bounds, nullptr, beam,
                       ldb, as_stream(stream));
+  if (storage != BP_STORAGE_F32 && staged_serves(t, BP_STORAGE_F32, false))
+    return run_staged_expanded(t, traces, storage, scales, T, lpad, pitch, out_of_bounds,
+                               nullptr, beam, ldb, as_stream(stream));
   return run_direct(traces, storage, scales, T, lpad, pitch, t->delays, t->weights, t->minmax,
                     t->info.n_sources, t->info.n_stations, t->info.n_phases, out_of_bounds,
                     nullptr, beam, ldb, as_stream(stream));
@@ -1337,7 +1379,7 @@ int bp_batch_create(const bp_table* const* tables, int n_tables, const bp_record
       const int c = i < 0 ? pref : order[i];
       bool all = true;
       for (int j = 0; j < n_tables; ++j)
-        if (tables[j] && tables[j]->info.uses_window_kernel &&
+        if (tables[j] && staged_serves(tables[j], storage, true) &&
             !config_fits(tables[j], c, storage, true))
           all = false;
       if (all) cfg = c;
@@ -1347,7 +1389,7 @@ int bp_batch_create(const bp_table* const* tables, int n_tables, const bp_record
   // one max-buffer row per warp only if every table leaves room for it
   int red_rows = cfg_of(cfg).ws;
   for (int j = 0; j < n_tables; ++j)
-    if (tables[j] && tables[j]->info.uses_window_kernel)
+    if (tables[j] && staged_serves(tables[j], storage, true))
       red_rows = std::min(red_rows, std::max(1, rows_for(tables[j], cfg, storage, true)));
   const int tt = cfg_time_tile(cfg);
   int rowcap = 0, max_active = 1;
@@ -1356,8 +1398,10 @@ int bp_batch_create(const bp_table* const* tables, int n_tables, const bp_record
   for (int i = 0; i < n_tables; ++i) {
     const bp_table* t = tables[i];
     if (!t) return fail(BP_ERR_INVALID_ARGUMENT, "NULL table %d", i);
-    if (!t->info.uses_window_kernel)
-      return fail(BP_ERR_UNSUPPORTED, "table %d needs the direct kernel; batches use the staged one", i);
+    if (!staged_serves(t, storage, true))
+      return fail(BP_ERR_UNSUPPORTED,
+                  "table %d needs the direct kernel with this storage; batches use the staged one",
+                  i);
     if (t->dev.P != P) return fail(BP_ERR_INVALID_ARGUMENT, "tables of a batch share n_phases");
     if (t->device != dev) return fail(BP_ERR_INVALID_ARGUMENT, "table %d is on another device", i);
     rowcap = std::max(rowcap, rowcap_for(t, cfg));
@@ -1527,8 +1571,9 @@ int bp_record_beamform_max_dev(const bp_table* t, const bp_record* q, int storag
   BP_NVTX("bp_record_beamform_max_dev");
   g_last_error.clear();
   if (!t || !q || !keys) return fail(BP_ERR_INVALID_ARGUMENT, "NULL argument");
-  if (!t->info.uses_window_kernel)
-    return fail(BP_ERR_UNSUPPORTED, "records need a table that uses the staged kernel");
+  if (!staged_serves(t, storage, true))
+    return fail(BP_ERR_UNSUPPORTED,
+                "records need a table that the staged kernel serves with this storage");
   if (q->station_mask) return fail(BP_ERR_INVALID_ARGUMENT, "station masks need a batch");
   if (q->out_of_bounds != 0 && q->out_of_bounds != 1)
     return fail(BP_ERR_INVALID_ARGUMENT, "out_of_bounds must be 0 or 1");
@@ -1622,7 +1667,7 @@ int bp_table_kernel_config(const bp_table* t, int storage, int reduce) {
   if (!t) return fail(BP_ERR_INVALID_ARGUMENT, "NULL table");
   if (storage < 0 || storage > 2 || (reduce != BP_REDUCE_MAX && reduce != BP_REDUCE_NONE))
     return fail(BP_ERR_INVALID_ARGUMENT, "bad storage / reduce");
-  if (!t->info.uses_window_kernel) return -1;
+  if (!staged_serves(t, storage, reduce == BP_REDUCE_MAX)) return -1;
   return config_for(t, storage, reduce == BP_REDUCE_MAX);
 }
 

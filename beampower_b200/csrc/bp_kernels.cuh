@@ -1605,6 +1605,20 @@ __global__ void prestack_h16_kernel(const float* __restrict__ F, const float* __
   }
 }
 
+// 16-bit trace rows back to FP32 rows of the same layout: element x of row
+// (s, p) becomes value * scale_s, exact (a 16-bit value times a power of
+// two).  Only copy 0 of the four shifted copies is read.  Lets the FP32
+// staged kernel serve 16-bit traces whose four-copy windows fit no shape.
+template <int STORAGE>
+__global__ void expand_h16_kernel(const void* __restrict__ in, const float* __restrict__ scales,
+                                  int P, long long pitch, float* __restrict__ out) {
+  const long long x = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int row = blockIdx.y;  // s * P + p
+  if (x >= pitch) return;
+  const float v = load_trace<STORAGE>(in, (size_t)row * kHalfCopies * pitch + x);
+  out[(size_t)row * pitch + x] = v * __ldg(scales + row / P);
+}
+
 #endif  // BP_TEMPLATE_KERNELS_ONLY
 
 }  // namespace bp

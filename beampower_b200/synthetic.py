@@ -63,7 +63,13 @@ LARGE = NetworkSpec("large-400k-src-60-sta-180000-samples", 60, 150.0, 50.0,
 SMALL_HEAVY = NetworkSpec("small-heavy-tailed", 20, 50.0, 25.0, 6000,
                           (20, 20, 10), 20.0, 3, noise="student_t3")
 
-SPECS = {s.name: s for s in (SMALL, LARGE, SMALL_HEAVY)}
+# A regional network: 64,000 sources ~10 km apart over 800 x 800 km, 100 Hz,
+# so that a tile's delay windows span 1,000-2,000 samples (wider than the
+# 16-bit default kernel shape holds).
+REGIONAL = NetworkSpec("regional-64k-src-60-sta-120000-samples", 60, 800.0, 100.0,
+                       120_000, (80, 80, 10), 40.0, 5)
+
+SPECS = {s.name: s for s in (SMALL, LARGE, SMALL_HEAVY, REGIONAL)}
 
 
 def _smooth(x: np.ndarray, width: int) -> np.ndarray:

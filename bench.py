@@ -1030,13 +1030,15 @@ def run_shapes(args, local_rank):
     """Kernel time of every compiled shape of the staged kernel, per trace
     storage, through the autotuner (beampower_b200.autotune): on the
     400,000-source table of the large workload (60 stations, 180,000
-    samples) and on the 50,000-source grid of the batch workload (100
-    stations) with one 90,000-sample window over all stations.  Shapes whose
-    shared memory does not fit a table are reported as None."""
+    samples), on the 50,000-source grid of the batch workload (100
+    stations) with one 90,000-sample window over all stations, and on a
+    regional network whose delay windows are wider than the 16-bit default
+    shape holds (64,000 sources, 800 km, 100 Hz, 120,000 samples).  Shapes
+    whose shared memory does not fit a table are reported as None."""
     import torch
     from beampower_b200 import autotune
     from beampower_b200.core import load_library
-    from beampower_b200.synthetic import (make_batch_workload, window_features,
+    from beampower_b200.synthetic import (REGIONAL, make_batch_workload, window_features,
                                           nominal_terms)
     from beampower_b200.tables import TravelTimeTable
     torch.cuda.set_device(local_rank)
@@ -1050,6 +1052,9 @@ def run_shapes(args, local_rank):
     cases = [("large-400k-src-60-sta-180000-samples", wl["time_delays"], wl["weights_sources"],
               wl["waveform_features"], wl["weights_phases"]),
              ("batch-grid-50k-src-100-sta-90000-samples", D50, W50, F50, bw["weights_phases"])]
+    rg = make_workload(REGIONAL)
+    cases.append((REGIONAL.name, rg["time_delays"], rg["weights_sources"],
+                  rg["waveform_features"], rg["weights_phases"]))
     out = {"shapes": dict(autotune.configs()), "tables": {}}
     sampler = ClockSampler(local_rank)
     sampler.start()
@@ -1066,6 +1071,17 @@ def run_shapes(args, local_rank):
             lib.bp_set_kernel_config(tr.storage, 1, -1)
             res["storages"][stg]["default"] = lib.bp_table_kernel_config(
                 table.handle, tr.storage, 1)
+            # the library's own choice (a staged shape, or the direct kernel
+            # where no shape holds the table's windows), timed the same way
+            table.beamform_max(tr, 0)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(2):
+                table.beamform_max(tr, 0)
+            e1.record()
+            torch.cuda.synchronize()
+            res["storages"][stg]["default_ms"] = e0.elapsed_time(e1) / 2
             del tr
         out["tables"][name] = res
         table.close()

@@ -220,3 +220,44 @@ def test_wide_windows_fall_back_correctly(cuda, bplib, oracle_lib):
         assert np.array_equal(am, ref[1]), c
     assert {1, 2, 8} & used  # a 16-warp shape ran (with the single atomic row)
     table.close()
+
+
+def _dequantized(tr, S, P):
+    """(S, T, P) float32 traces from 16-bit rows: copy 0 times the station's
+    (power-of-two) scale, exact."""
+    from beampower_b200.core import trace_copies
+    T = tr.n_samples
+    rows = tr.buf[0::trace_copies(tr.storage)].float().cpu().numpy()[:, tr.lpad:tr.lpad + T]
+    V = rows.reshape(S, P, T) * tr.scales.cpu().numpy().astype(np.float32)[:, None, None]
+    return np.ascontiguousarray(V.astype(np.float32).transpose(0, 2, 1))
+
+
+@pytest.mark.parametrize("unit", [True, False])
+def test_windows_too_wide_for_16bit_rings(cuda, bplib, oracle_lib, unit):
+    """Delay windows of ~4,500 samples: FP32 rings still fit a staged shape,
+    the four 16-bit copies of every window fit none.  FP32 calls run the
+    staged kernel; 16-bit calls expand their traces to FP32 (value times the
+    power-of-two scale, exact) and run the same FP32 shapes, so both equal
+    the oracle bit for bit -- the 16-bit ones on the dequantized traces."""
+    from beampower_b200.tables import TravelTimeTable
+    S, P = 6, 2
+    F, A, D, W = _network(60, S=S, P=P, N=300, T=12000, unit=unit, spread=4500)
+    table = TravelTimeTable(D, W)
+    assert table.info["uses_window_kernel"] == 1
+    assert table.info["max_spread"] > 4000
+    assert bplib.bp_table_kernel_config(table.handle, 0, 1) >= 0
+    for st in (1, 2):
+        assert bplib.bp_table_kernel_config(table.handle, st, 1) == -1
+        assert bplib.bp_table_kernel_config(table.handle, st, 0) == -1
+    for storage in ("fp32", "fp16", "bf16"):
+        tr = table.traces_from_features(F, A, storage=storage)
+        U = oracle_lib.prestack(F, A) if storage == "fp32" else _dequantized(tr, S, P)
+        for oob in (0, 1):
+            ref_bm, ref_am = oracle_lib.beamform_max(U, D, W, oob)
+            bm, am = _run(table, tr, oob, "max")
+            assert np.array_equal(bm.view(np.uint32), ref_bm.view(np.uint32)), (storage, oob)
+            assert np.array_equal(am, ref_am), (storage, oob)
+            ref_full = oracle_lib.beamform(U, D, W, oob)
+            beam = _run(table, tr, oob, "none")
+            assert np.array_equal(beam.view(np.uint32), ref_full.view(np.uint32)), (storage, oob)
+    table.close()
