@@ -860,32 +860,47 @@ int bp_traces_from_prestacked_dev(const float* U, size_t T, size_t S, size_t P, 
 }
 
 // 16-bit traces of a table whose four-copy windows fit no staged shape while
-// its FP32 windows do: the rows are expanded to FP32 in a scratch buffer
-// (value * scale_s, exact) and the FP32 staged kernel runs on them.  Per term
-// it forms round(w * (u * scale_s)) and adds it with one rounding, stations
-// then phases ascending: the value and order of the direct kernel's 16-bit
-// path, at the staged kernel's speed.
+// its FP32 windows do are expanded to FP32 rows of the same layout in a
+// scratch buffer (value * scale_s, exact), and the FP32 staged kernel runs on
+// them.  Per term it forms round(w * (u * scale_s)) and adds it with one
+// rounding, stations then phases ascending: the value and order of the direct
+// kernel's 16-bit path, at the staged kernel's speed.
+struct ScratchF32 {
+  float* p = nullptr;
+  cudaStream_t s = nullptr;
+  ~ScratchF32() {
+    if (p) cudaFreeAsync(p, s);
+  }
+};
+
+static bool expands_to_f32(const bp_table* t, int storage, bool maxred) {
+  return storage != BP_STORAGE_F32 && !staged_serves(t, storage, maxred) &&
+         staged_serves(t, BP_STORAGE_F32, maxred);
+}
+
+static int expand_to_f32(const bp_table* t, const void* traces, int storage,
+                         const float* scales, size_t pitch, cudaStream_t st, ScratchF32* out) {
+  const int S = t->dev.S, P = t->dev.P;
+  out->s = st;
+  BP_CUDA(cudaMallocAsync(&out->p, (size_t)S * P * pitch * sizeof(float), st));
+  const dim3 grid((unsigned)((pitch + 255) / 256), (unsigned)(S * P));
+  if (storage == BP_STORAGE_BF16)
+    bp::expand_h16_kernel<BP_STORAGE_BF16><<<grid, 256, 0, st>>>(traces, scales, P,
+                                                                 (long long)pitch, out->p);
+  else
+    bp::expand_h16_kernel<BP_STORAGE_F16><<<grid, 256, 0, st>>>(traces, scales, P,
+                                                                (long long)pitch, out->p);
+  BP_LAUNCHED("expand_h16_kernel");
+  return BP_OK;
+}
+
 static int run_staged_expanded(const bp_table* t, const void* traces, int storage,
                                const float* scales, size_t T, size_t lpad, size_t pitch,
                                int out_of_bounds, unsigned long long* keys, float* beam,
                                size_t ldb, cudaStream_t st) {
-  const int S = t->dev.S, P = t->dev.P;
-  float* f32 = nullptr;
-  BP_CUDA(cudaMallocAsync(&f32, (size_t)S * P * pitch * sizeof(float), st));
-  struct Scratch32 {
-    float* p;
-    cudaStream_t s;
-    ~Scratch32() { cudaFreeAsync(p, s); }
-  } guard{f32, st};
-  const dim3 grid((unsigned)((pitch + 255) / 256), (unsigned)(S * P));
-  if (storage == BP_STORAGE_BF16)
-    bp::expand_h16_kernel<BP_STORAGE_BF16><<<grid, 256, 0, st>>>(traces, scales, P,
-                                                                 (long long)pitch, f32);
-  else
-    bp::expand_h16_kernel<BP_STORAGE_F16><<<grid, 256, 0, st>>>(traces, scales, P,
-                                                                (long long)pitch, f32);
-  BP_LAUNCHED("expand_h16_kernel");
-  return run_staged(t, f32, BP_STORAGE_F32, nullptr, T, lpad, pitch, out_of_bounds, keys, beam,
+  ScratchF32 f32;
+  if (int rc = expand_to_f32(t, traces, storage, scales, pitch, st, &f32)) return rc;
+  return run_staged(t, f32.p, BP_STORAGE_F32, nullptr, T, lpad, pitch, out_of_bounds, keys, beam,
                     ldb, st);
 }
 
@@ -897,7 +912,7 @@ static int max_keys(const bp_table* t, const void* traces, int storage, const fl
   if (staged_serves(t, storage, true))
     return run_staged(t, traces, storage, scales, T, lpad, pitch, out_of_bounds, keys, nullptr,
                       0, st);
-  if (storage != BP_STORAGE_F32 && staged_serves(t, BP_STORAGE_F32, true))
+  if (expands_to_f32(t, storage, true))
     return run_staged_expanded(t, traces, storage, scales, T, lpad, pitch, out_of_bounds, keys,
                                nullptr, 0, st);
   return run_direct(traces, storage, scales, T, lpad, pitch, t->delays, t->weights, t->minmax,
@@ -949,7 +964,7 @@ int bp_beamform_dev(const bp_table* t, const void* traces, int storage, const fl
   if (staged_serves(t, storage, false))
     return run_staged(t, traces, storage, scales, T, lpad, pitch, out_of_bounds, nullptr, beam,
                       ldb, as_stream(stream));
-  if (storage != BP_STORAGE_F32 && staged_serves(t, BP_STORAGE_F32, false))
+  if (expands_to_f32(t, storage, false))
     return run_staged_expanded(t, traces, storage, scales, T, lpad, pitch, out_of_bounds,
                                nullptr, beam, ldb, as_stream(stream));
   return run_direct(traces, storage, scales, T, lpad, pitch, t->delays, t->weights, t->minmax,
@@ -1571,9 +1586,9 @@ int bp_record_beamform_max_dev(const bp_table* t, const bp_record* q, int storag
   BP_NVTX("bp_record_beamform_max_dev");
   g_last_error.clear();
   if (!t || !q || !keys) return fail(BP_ERR_INVALID_ARGUMENT, "NULL argument");
-  if (!staged_serves(t, storage, true))
-    return fail(BP_ERR_UNSUPPORTED,
-                "records need a table that the staged kernel serves with this storage");
+  const bool expand = expands_to_f32(t, storage, true);
+  if (!expand && !staged_serves(t, storage, true))
+    return fail(BP_ERR_UNSUPPORTED, "records need a table that the staged kernel serves");
   if (q->station_mask) return fail(BP_ERR_INVALID_ARGUMENT, "station masks need a batch");
   if (q->out_of_bounds != 0 && q->out_of_bounds != 1)
     return fail(BP_ERR_INVALID_ARGUMENT, "out_of_bounds must be 0 or 1");
@@ -1586,11 +1601,16 @@ int bp_record_beamform_max_dev(const bp_table* t, const bp_record* q, int storag
   if (n_out == 0) return BP_OK;
   cudaStream_t st = as_stream(stream);
   BP_CUDA(cudaMemsetAsync(keys, 0, n_out * sizeof(unsigned long long), st));
+  ScratchF32 f32;
+  if (expand) {
+    if (int rc = expand_to_f32(t, q->traces, storage, q->scales, q->pitch, st, &f32)) return rc;
+    storage = BP_STORAGE_F32;
+  }
   bp::LaunchArgs a{};
   a.tab0 = table_view(t);
   bp::RecordView& r = a.rec0;
-  r.traces = q->traces;
-  r.scales = q->scales;
+  r.traces = expand ? static_cast<const void*>(f32.p) : q->traces;
+  r.scales = expand ? nullptr : q->scales;
   r.pitch = (long long)q->pitch;
   r.t_origin = q->t_origin;
   r.lpad = (int)q->lpad;

@@ -135,7 +135,8 @@ typedef struct bp_table_info {
   int32_t max_spread;        /* widest per-tile station delay window - 1   */
   int32_t max_active;        /* most active stations in one tile           */
   int32_t any_nonfinite;     /* some non-zero weight is NaN or +-inf       */
-  int32_t uses_window_kernel;/* 1: staged kernel, 0: direct kernel         */
+  int32_t uses_window_kernel;/* 1: staged kernel (FP32 windows fit a shape),
+                                 0: direct kernel for every storage        */
 } bp_table_info;
 
 /* Build a table from device arrays (N, S, P) int32 and (N, S) float32.
@@ -454,8 +455,12 @@ BP_API int bp_set_kernel_config(int storage, int reduce, int config);
 BP_API int bp_get_kernel_config(int storage, int reduce);
 /* The shape a call on this table runs with (storage, reduce): the chosen one
  * when its shared memory and blocks per SM fit the table, else the first
- * that fits in a fixed, measured order; -1 when the table uses the direct
- * kernel, a negative error code for bad arguments. */
+ * that fits in a fixed, measured order; -1 when no shape holds the table's
+ * windows in this storage (16-bit calls then expand their traces to FP32 and
+ * run the FP32 shape, with the direct kernel's values, when that fits; else,
+ * and for tables with uses_window_kernel == 0, the direct kernel runs); a
+ * negative error code for bad arguments.  Records expand the same way;
+ * batches need a shape for their own storage. */
 BP_API int bp_table_kernel_config(const bp_table *table, int storage, int reduce);
 
 /* ---- diagnostics -------------------------------------------------------- */

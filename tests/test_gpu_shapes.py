@@ -261,3 +261,26 @@ def test_windows_too_wide_for_16bit_rings(cuda, bplib, oracle_lib, unit):
             beam = _run(table, tr, oob, "none")
             assert np.array_equal(beam.view(np.uint32), ref_full.view(np.uint32)), (storage, oob)
     table.close()
+
+
+def test_stream_on_windows_too_wide_for_16bit_rings(cuda, oracle_lib):
+    """A 16-bit stream on the same kind of table runs through the FP32
+    expansion, record by record (each record keeps its own station scales),
+    and stays within the FP16 tolerance of the FP32 offline result."""
+    import torch
+    from beampower_b200.stream import NetworkStream
+    from beampower_b200.tables import TravelTimeTable
+    S, P = 6, 2
+    F, A, D, W = _network(61, S=S, P=P, N=300, T=12000, unit=True, spread=4500)
+    table = TravelTimeTable(D, W)
+    ref_bm, _ = oracle_lib.beamform_max(oracle_lib.prestack(F, A), D, W, 0)
+    ns = NetworkStream(table, A, storage="fp16")
+    for a in range(0, F.shape[2], 5000):
+        ns.push(F[:, :, a:a + 5000])
+    ns.flush()
+    bm, _ = ns.collect()
+    torch.cuda.synchronize()
+    assert bm.shape == ref_bm.shape
+    tol = 1e-3 * float(np.abs(ref_bm).max())
+    assert np.all(np.abs(bm - ref_bm) <= tol)
+    table.close()
