@@ -71,7 +71,12 @@ class WindowBatch:
         trace bytes and stays within 1e-3 of a float64 beam (11 significant
         bits: at most two roundings of 2^-11 per term of one sign); FP32
         gives the reference's bits; BF16 (8 significant bits) cannot promise
-        1e-3 (one rounding alone is up to 2^-8 = 3.9e-3).
+        1e-3 (one rounding alone is up to 2^-8 = 3.9e-3).  A table whose
+        delay windows are too wide for the four 16-bit copies of every
+        window in any kernel shape, while its FP32 windows fit one, makes
+        the batch store FP32 (``self.storage`` says which): those traces
+        take half the bytes of the 16-bit copies, run at the same speed and
+        give the reference's bits.
     """
 
     def __init__(self, tables, windows, weights_phases, storage="fp16", stream=None):
@@ -81,8 +86,12 @@ class WindowBatch:
         self.tables = list(tables)
         self.windows = list(windows)
         self.device = self.tables[0].device
-        self.storage = storage
         st = STORAGE[storage]
+        if st != 0 and any(self.lib.bp_table_kernel_config(t.handle, st, 1) < 0
+                           and self.lib.bp_table_kernel_config(t.handle, 0, 1) >= 0
+                           for t in self.tables):
+            storage, st = "fp32", 0
+        self.storage = storage
         P = self.tables[0].n_phases
         self.alpha = _dev_tensor(weights_phases, torch.float32, self.device)
         S, C, _ = self.alpha.shape

@@ -284,3 +284,24 @@ def test_stream_on_windows_too_wide_for_16bit_rings(cuda, oracle_lib):
     tol = 1e-3 * float(np.abs(ref_bm).max())
     assert np.all(np.abs(bm - ref_bm) <= tol)
     table.close()
+
+
+def test_batch_on_windows_too_wide_for_16bit_rings(cuda, oracle_lib):
+    """A 16-bit batch that holds such a table stores FP32 traces instead
+    (no 16-bit shape fits it) and gives the oracle's bits."""
+    import torch
+    from beampower_b200.batch import Window, WindowBatch
+    from beampower_b200.tables import TravelTimeTable
+    S, P = 6, 2
+    F, A, D, W = _network(62, S=S, P=P, N=300, T=12000, unit=True, spread=4500)
+    table = TravelTimeTable(D, W)
+    batch = WindowBatch([table], [Window(0, F.shape[2])], A, storage="fp16")
+    assert batch.storage == "fp32"
+    batch.set_features(0, F)
+    (bm, am), = batch.run()
+    torch.cuda.synchronize()
+    ref_bm, ref_am = oracle_lib.beamform_max(oracle_lib.prestack(F, A), D, W, 0)
+    assert np.array_equal(bm.cpu().numpy().view(np.uint32), ref_bm.view(np.uint32))
+    assert np.array_equal(am.cpu().numpy(), ref_am)
+    batch.close()
+    table.close()
