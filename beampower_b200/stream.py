@@ -54,7 +54,11 @@ class NetworkStream:
     out_of_bounds: 'strict' or 'flexible'
     storage: 'fp16' (default: within 1e-3 of a float64 beam), 'fp32' (the
         reference's bits; streamed output equals the offline call bit for
-        bit) or 'bf16' (within 4e-3)
+        bit) or 'bf16' (within 4e-3).  A table whose delay windows are too
+        wide for the four 16-bit copies of every window in any kernel shape,
+        while its FP32 windows fit one, makes the stream store FP32
+        (``self.storage`` says which): half the bytes, the same speed, the
+        reference's bits.
     """
 
     def __init__(self, table: TravelTimeTable, weights_phases, out_of_bounds="strict",
@@ -68,6 +72,10 @@ class NetworkStream:
         self.alpha = _dev_tensor(weights_phases, torch.float32, self.device)
         self.S, self.C, self.P = map(int, self.alpha.shape)
         self.oob = 0 if out_of_bounds == "strict" else 1
+        if (STORAGE[storage] != 0
+                and self.lib.bp_table_kernel_config(table.handle, STORAGE[storage], 1) < 0
+                and self.lib.bp_table_kernel_config(table.handle, 0, 1) >= 0):
+            storage = "fp32"
         self.storage = storage
         self._st = STORAGE[storage]
         info = table.info

@@ -263,26 +263,46 @@ def test_windows_too_wide_for_16bit_rings(cuda, bplib, oracle_lib, unit):
     table.close()
 
 
-def test_stream_on_windows_too_wide_for_16bit_rings(cuda, oracle_lib):
-    """A 16-bit stream on the same kind of table runs through the FP32
-    expansion, record by record (each record keeps its own station scales),
-    and stays within the FP16 tolerance of the FP32 offline result."""
+def test_stream_on_windows_too_wide_for_16bit_rings(cuda, bplib, oracle_lib):
+    """A 16-bit stream on such a table stores FP32 instead and equals the
+    oracle bit for bit; 16-bit records handed over directly are expanded to
+    FP32 (the record path of the same fallback)."""
+    import ctypes as ct
     import torch
+    from beampower_b200.core import Record, STORAGE, check
     from beampower_b200.stream import NetworkStream
-    from beampower_b200.tables import TravelTimeTable
+    from beampower_b200.tables import TravelTimeTable, _stream_ptr
     S, P = 6, 2
     F, A, D, W = _network(61, S=S, P=P, N=300, T=12000, unit=True, spread=4500)
     table = TravelTimeTable(D, W)
-    ref_bm, _ = oracle_lib.beamform_max(oracle_lib.prestack(F, A), D, W, 0)
+    U = oracle_lib.prestack(F, A)
+    ref_bm, ref_am = oracle_lib.beamform_max(U, D, W, 0)
     ns = NetworkStream(table, A, storage="fp16")
+    assert ns.storage == "fp32"
     for a in range(0, F.shape[2], 5000):
         ns.push(F[:, :, a:a + 5000])
     ns.flush()
-    bm, _ = ns.collect()
+    bm, am = ns.collect()
+    assert np.array_equal(bm.view(np.uint32), ref_bm.view(np.uint32))
+    assert np.array_equal(am, ref_am)
+    # one 16-bit record over the whole trace, through the C-ABI
+    tr = table.traces_from_features(F, A, storage="fp16")
+    T = F.shape[2]
+    bm16 = torch.zeros(T, dtype=torch.float32, device=tr.buf.device)
+    am16 = torch.zeros(T, dtype=torch.int32, device=tr.buf.device)
+    keys = torch.empty(T, dtype=torch.int64, device=tr.buf.device)
+    r = Record()
+    r.table, r.out_of_bounds = 0, 0
+    r.traces, r.scales = tr.buf.data_ptr(), tr.scales.data_ptr()
+    r.n_samples, r.lpad, r.pitch, r.t_origin, r.out0, r.out1 = T, tr.lpad, tr.pitch, 0, 0, T
+    r.station_mask = None
+    r.beam_max, r.argmax = bm16.data_ptr(), am16.data_ptr()
+    check(bplib.bp_record_beamform_max_dev(table.handle, ct.byref(r), STORAGE["fp16"],
+                                           keys.data_ptr(), _stream_ptr()))
     torch.cuda.synchronize()
-    assert bm.shape == ref_bm.shape
-    tol = 1e-3 * float(np.abs(ref_bm).max())
-    assert np.all(np.abs(bm - ref_bm) <= tol)
+    want_bm, want_am = oracle_lib.beamform_max(_dequantized(tr, S, P), D, W, 0)
+    assert np.array_equal(bm16.cpu().numpy().view(np.uint32), want_bm.view(np.uint32))
+    assert np.array_equal(am16.cpu().numpy(), want_am)
     table.close()
 
 
