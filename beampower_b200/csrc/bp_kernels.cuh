@@ -340,8 +340,9 @@ struct WindowSmem {
     st_lo = o;       o += (size_t)max_active * P * sizeof(int);
     st_w = o;        o += (size_t)max_active * P * sizeof(int);
     st_sc = o;       o += (size_t)max_active * sizeof(float);
-    o = align_up_sz(o, 8);
+    o = align_up_sz(o, 16);
     bars = o;        o += (size_t)2 * NSTAGE * sizeof(uint64_t);
+    o = align_up_sz(o, 16);    // the current item is an int4 at misc + 32
     misc = o;        o += 64;  // abort flag, active count, current item
     total = align_up_sz(o, 128);
   }
