@@ -44,6 +44,11 @@ def test_ctypes_table_covers_header():
     assert lib.bp_version().startswith(b"beampower_b200")
 
 
+def test_integration_guide_lists_every_symbol():
+    text = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    assert [s for s in declared_symbols() if f"`{s}`" not in text] == []
+
+
 def test_reference_argtypes_kept():
     """The drop-in argtypes equal beampower/core.py:65-87 (restype added)."""
     from beampower_b200.core import LIBRARIES
