@@ -1090,17 +1090,21 @@ int host_max_chunked(const float* F, const float* alpha, const int32_t* delays, 
   BP_CUDA(cudaMemsetAsync(d_keys, 0, T * sizeof(unsigned long long), st));
   // the allocations above are ordered on `st`; the upload stream waits for them
   std::vector<cudaEvent_t> ev(n_chunks + 1, nullptr);
+  // on every return: the upload stream too is drained before the tables and
+  // (after this guard) the buffers go -- an early return can leave a chunk's
+  // copies and table build queued there that `st` never waited for
   struct Cleanup {
     std::vector<cudaEvent_t>& ev;
     std::vector<bp_table*> tables;
-    cudaStream_t st;
+    cudaStream_t st, up;
     ~Cleanup() {
+      cudaStreamSynchronize(up);
       cudaStreamSynchronize(st);
       for (bp_table* t : tables) bp_table_destroy(t);
       for (cudaEvent_t e : ev)
         if (e) cudaEventDestroy(e);
     }
-  } cleanup{ev, {}, st};
+  } cleanup{ev, {}, st, up};
   for (auto& e : ev) BP_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   BP_CUDA(cudaEventRecord(ev[n_chunks], st));
   BP_CUDA(cudaStreamWaitEvent(up, ev[n_chunks], 0));
