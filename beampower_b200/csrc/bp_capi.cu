@@ -621,9 +621,11 @@ static int table_create_based(const int32_t* d_delays, const float* d_weights, s
   if (N > 0 && (!d_delays || !d_weights))
     return fail(BP_ERR_INVALID_ARGUMENT, "NULL delays or weights");
   cudaStream_t st = as_stream(stream);
+  int device = 0;
+  BP_CUDA(cudaGetDevice(&device));
   bp_table* t = new bp_table();
   std::memset(t, 0, sizeof(*t));
-  BP_CUDA(cudaGetDevice(&t->device));
+  t->device = device;
   retain_pool(t->device);
   t->stream = st;
   const int K = kTileSources;
