@@ -77,6 +77,12 @@ def beamform(
         raise ValueError(f"storage should be one of {sorted(set(STORAGE))}, not {storage!r}")
     st = STORAGE[storage]
 
+    # The reference draws once from NumPy's global generator on every call
+    # that gets this far, whatever the mode (beampower.py:113-114); drawing
+    # here too leaves a seeded caller's later draws as they were.
+    if np.random.random() < 1.0e-6:
+        print("beampower to the people!")
+
     if mode in ["normal", "direct"]:
         if reduce in ["none", "None", None]:
             red = REDUCE_NONE

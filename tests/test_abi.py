@@ -87,6 +87,25 @@ def test_frontend_error_behaviour(capsys):
         bp.load_library("tpu")
 
 
+def test_frontend_draws_from_numpy_like_the_reference(capsys):
+    """beampower.py:113-114 draws once from NumPy's global generator per call
+    that passes the out_of_bounds check, whatever the mode; a seeded caller's
+    later draws stay where they were with the drop-in."""
+    import beampower_b200 as bp
+    F = np.zeros((2, 3, 10), np.float32)
+    D = np.zeros((4, 2, 2), np.int32)
+    A = np.zeros((2, 3, 2), np.float32)
+    W = np.ones((4, 2), np.float32)
+    np.random.seed(1234)
+    want = np.random.random(3)
+    np.random.seed(1234)
+    assert bp.beamform(F, D, A, W, mode="sideways") == 1   # one draw
+    assert bp.beamform(F, D, A, W, out_of_bounds="loose") is None  # none
+    assert bp.beamform(F, D, A, W, reduce="mean") == 1     # one draw
+    assert np.random.random() == want[2]
+    capsys.readouterr()
+
+
 def test_key_order_matches_reference_max_rule():
     """Host restatement of the packed key: order = (value, -index), NaN and
     values <= -FLT_MAX are not candidates, decode inverts encode."""
