@@ -46,7 +46,11 @@ const char* cufft_name(cufftResult r) {
 
 // Plans are costly to make: kept per (device, length, batch, kind) for the
 // life of the process.  A plan holds one stream at a time, so setting its
-// stream and enqueueing its transform happen under the cache's lock.
+// stream and enqueueing its transform happen under the cache's lock.  The
+// lock orders the enqueues only: a plan's work area is shared by every stream
+// that uses it, so transforms of one shape on different streams must not
+// overlap on the GPU (stated in the header; the library's own callers use
+// one stream per call).
 struct PlanCache {
   std::mutex mu;
   std::map<std::tuple<int, int, int, int>, cufftHandle> plans;

@@ -385,7 +385,11 @@ BP_API int bp_detect_dev(const float *d_beam_max, const int32_t *d_argmax,
  * scratch with cudaMallocAsync on `stream`; cuFFT plans are cached per
  * (device, length, rows) for the life of the process. */
 
-/* d_x: n_rows rows of n_samples float32 (contiguous); d_out: same shape. */
+/* d_x: n_rows rows of n_samples float32 (contiguous); d_out: same shape.
+ * The FFT plans behind the envelope are cached per (device, length, rows)
+ * and shared by every stream: envelope calls of the same shape on different
+ * streams must not overlap on the GPU (order them with an event or run them
+ * on one stream); calls on one stream are always safe. */
 BP_API int bp_envelope_dev(const float *d_x, size_t n_rows, size_t n_samples, float clip_max,
                            float *d_out, void *stream);
 
