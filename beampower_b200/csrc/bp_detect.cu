@@ -166,8 +166,10 @@ __global__ void pw_inner_kernel(const int4* __restrict__ inner, const int* __res
 // segments of `len` values starting every seg_stride values.
 // Split trees of the lengths seen so far, built and uploaded once per device
 // and kept for the life of the process (up to kTreeCache lengths; beyond
-// that a tree is uploaded into the call's scratch).  The upload is
-// synchronous, so a cached tree is complete before any stream uses it.
+// that a tree is uploaded into the call's scratch).  The upload is ordered
+// on the call's stream and waited for (a plain cudaMemcpy from pageable
+// memory may return before its DMA lands), so a cached tree is complete
+// before any stream uses it.
 struct DevTree {
   int n_leaves = 0, n_inner = 0, n_levels = 0, n_nodes = 0, root = 0;
   const int4* leaves = nullptr;
@@ -178,7 +180,7 @@ constexpr size_t kTreeCache = 64;
 std::mutex g_tree_mu;
 std::map<std::pair<int, int>, DevTree> g_trees;
 
-int upload_tree(const PwTree& t, DevTree* d, void* mem) {
+int upload_tree(const PwTree& t, DevTree* d, void* mem, cudaStream_t st) {
   char* p = static_cast<char*>(mem);
   d->n_leaves = (int)t.leaves.size();
   d->n_inner = (int)t.inner.size();
@@ -189,15 +191,18 @@ int upload_tree(const PwTree& t, DevTree* d, void* mem) {
   d->inner = reinterpret_cast<const int4*>(p + t.leaves.size() * sizeof(int4));
   d->levels = reinterpret_cast<const int*>(p + (t.leaves.size() + t.inner.size()) *
                                                    sizeof(int4));
-  BP_CUDA(cudaMemcpy(p, t.leaves.data(), t.leaves.size() * sizeof(int4),
-                     cudaMemcpyHostToDevice));
+  BP_CUDA(cudaMemcpyAsync(p, t.leaves.data(), t.leaves.size() * sizeof(int4),
+                          cudaMemcpyHostToDevice, st));
   if (!t.inner.empty()) {
-    BP_CUDA(cudaMemcpy(p + t.leaves.size() * sizeof(int4), t.inner.data(),
-                       t.inner.size() * sizeof(int4), cudaMemcpyHostToDevice));
-    BP_CUDA(cudaMemcpy(p + (t.leaves.size() + t.inner.size()) * sizeof(int4),
-                       t.level_end.data(), t.level_end.size() * sizeof(int),
-                       cudaMemcpyHostToDevice));
+    BP_CUDA(cudaMemcpyAsync(p + t.leaves.size() * sizeof(int4), t.inner.data(),
+                            t.inner.size() * sizeof(int4), cudaMemcpyHostToDevice, st));
+    BP_CUDA(cudaMemcpyAsync(p + (t.leaves.size() + t.inner.size()) * sizeof(int4),
+                            t.level_end.data(), t.level_end.size() * sizeof(int),
+                            cudaMemcpyHostToDevice, st));
   }
+  // the host vectors are freed on return and a cached tree is shared by
+  // every stream: wait until the copies have landed
+  BP_CUDA(cudaStreamSynchronize(st));
   return BP_OK;
 }
 
@@ -229,7 +234,7 @@ int get_tree(int len, DevTree* out, Scratch& sc) {
   if (g_trees.size() < kTreeCache) {
     BP_CUDA(cudaMalloc(&mem, tree_bytes(t)));
     DevTree d;
-    if (int rc = upload_tree(t, &d, mem)) {
+    if (int rc = upload_tree(t, &d, mem, sc.st)) {
       cudaFree(mem);
       return rc;
     }
@@ -239,8 +244,7 @@ int get_tree(int len, DevTree* out, Scratch& sc) {
   }
   char* scratch = nullptr;  // cache full: this call's own copy
   BP_TRY(sc.get(&scratch, tree_bytes(t)));
-  BP_CUDA(cudaStreamSynchronize(sc.st));  // the scratch is stream-ordered
-  return upload_tree(t, out, scratch);
+  return upload_tree(t, out, scratch, sc.st);  // ordered after the allocation
 }
 
 int pw_mean(const float* x, long long seg_stride, int len, int n_seg, int mode,
