@@ -103,3 +103,20 @@ def test_differential_matches_reference(oracle_lib, ref, seed):
     want = ref.beamform_differential(U, D, W, num_threads=1)
     got = oracle_lib.beamform_differential(U, D, W)
     assert np.array_equal(_bits(got), _bits(want))
+
+
+@pytest.mark.parametrize("seed", SEEDS)
+def test_sampled_max_matches_full_max(oracle_lib, ref, seed):
+    """The oracle's max at chosen samples (the checker of the full-size GPU
+    tests) equals the reference's max over the whole record at those
+    samples, including samples without a candidate (0 and index 0)."""
+    F, A, D, W = _case(seed, non_negative=True)
+    U = ref.prestack(F, A)
+    T = U.shape[1]
+    rng = np.random.default_rng(seed)
+    times = np.unique(np.concatenate([[0, T - 1], rng.integers(0, T, size=min(T, 25))]))
+    for oob in (0, 1):
+        bm_r, am_r = ref.beamform_max(U, D, W, oob, num_threads=3)
+        bm, am = oracle_lib.beamform_max_at(U, D, W, times, oob)
+        assert np.array_equal(_bits(bm), _bits(bm_r[times])), oob
+        assert np.array_equal(am, am_r[times]), oob
