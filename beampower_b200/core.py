@@ -66,7 +66,6 @@ class Record(ct.Structure):
     ]
 
 
-# symbol -> (argtypes, restype)
 class PeakOptions(ct.Structure):
     """bp_peak_options (include/beampower_b200.h)."""
 
@@ -91,6 +90,7 @@ class PeakOptions(ct.Structure):
     ]
 
 
+# symbol -> (argtypes, restype)
 SIGNATURES = {
     # drop-ins, argtypes of beampower/core.py:65-87 (restype added: int status)
     "beamform": ([_f32p, _i32p, _f32p, _sz, _sz, _sz, _sz, _int, _f32p], _int),

@@ -193,3 +193,45 @@ def test_cmake_project_configures(tmp_path):
                        text=True, timeout=300)
     assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
     assert (tmp_path / "CMakeCache.txt").exists()
+
+
+def _c_kind(decl):
+    """Kind of a C parameter / return declaration: ptr, u64, i64, i32, f32, f64."""
+    d = decl.replace("const", " ").strip()
+    if "*" in d:
+        return "ptr"
+    base = " ".join(d.split()[:-1]) if len(d.split()) > 1 and d.split()[-1] not in (
+        "int", "float", "double", "size_t") else d
+    base = " ".join(base.split())
+    return {"size_t": "u64", "uint64_t": "u64", "unsigned long long": "u64",
+            "int64_t": "i64", "long long": "i64", "int": "i32", "int32_t": "i32",
+            "float": "f32", "double": "f64"}[base]
+
+
+def _ctypes_kind(t):
+    if t is None:
+        return None
+    if issubclass(t, (ct._Pointer, ct.c_void_p, ct.c_char_p)):
+        return "ptr"
+    if t in (ct.c_float, ct.c_double):
+        return "f32" if t is ct.c_float else "f64"
+    signed = t(-1).value == -1
+    return {(8, False): "u64", (8, True): "i64", (4, True): "i32"}[(ct.sizeof(t), signed)]
+
+
+def test_ctypes_signatures_match_header_prototypes():
+    """Every SIGNATURES entry has the header prototype's argument count and
+    the same kind (pointer, 32/64-bit integer, float, double) per argument
+    and for the result, so a drifted table cannot pass arguments silently."""
+    from beampower_b200.core import SIGNATURES
+    text = "\n".join(open(h).read() for h in glob.glob(os.path.join(ROOT, "include", "*.h")))
+    text = re.sub(r"/\*.*?\*/", " ", text, flags=re.S)
+    protos = re.findall(r"BP_API\s+([\w\s\*]+?)\b(\w+)\s*\(([^)]*)\)\s*;", text)
+    assert len(protos) == len(declared_symbols())
+    for ret, name, params in protos:
+        args = [p for p in (x.strip() for x in params.split(",")) if p and p != "void"]
+        argtypes, restype = SIGNATURES[name]
+        assert len(args) == len(argtypes), name
+        for i, (a, t) in enumerate(zip(args, argtypes)):
+            assert _c_kind(a) == _ctypes_kind(t), f"{name} argument {i}: {a}"
+        assert _c_kind(ret + " r") == _ctypes_kind(restype), f"{name} result"
