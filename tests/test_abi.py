@@ -235,3 +235,34 @@ def test_ctypes_signatures_match_header_prototypes():
         for i, (a, t) in enumerate(zip(args, argtypes)):
             assert _c_kind(a) == _ctypes_kind(t), f"{name} argument {i}: {a}"
         assert _c_kind(ret + " r") == _ctypes_kind(restype), f"{name} result"
+
+
+def test_struct_mirrors_match_header_layout(tmp_path):
+    """The ctypes mirrors of bp_table_info, bp_record and bp_peak_options have
+    the header structs' size and every field at the header's offset: a C
+    program built from the header by gcc prints them."""
+    import shutil
+    import subprocess
+    from beampower_b200.core import PeakOptions, Record, TableInfo
+    gcc = shutil.which("gcc") or shutil.which("cc")
+    if gcc is None:
+        pytest.skip("no C compiler")
+    mirrors = {"bp_table_info": TableInfo, "bp_record": Record, "bp_peak_options": PeakOptions}
+    lines = ["#include <stdio.h>", "#include <stddef.h>", '#include "beampower_b200.h"',
+             "int main(void) {"]
+    for cname, st in mirrors.items():
+        lines.append(f'  printf("{cname} size %zu\\n", sizeof({cname}));')
+        for field, _ in st._fields_:
+            lines.append(f'  printf("{cname} {field} %zu\\n", offsetof({cname}, {field}));')
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run([gcc, "-std=c99", "-I", os.path.join(ROOT, "include"), str(src), "-o",
+                    str(exe)], check=True, capture_output=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout
+    got = {(a, b): int(c) for a, b, c in (ln.split() for ln in out.splitlines())}
+    for cname, st in mirrors.items():
+        assert got[(cname, "size")] == ct.sizeof(st), cname
+        for field, _ in st._fields_:
+            assert got[(cname, field)] == getattr(st, field).offset, f"{cname}.{field}"
