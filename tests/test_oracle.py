@@ -119,3 +119,15 @@ def test_known_answer_nan_never_wins(oracle_lib):
     bm, am = oracle_lib.beamform_max(U, D, W, 0)
     assert am[5] == 0 and bm[5] == 0.0                    # NaN beams are not candidates
     assert np.all(am[np.arange(T) != 5] == 0)
+
+
+def test_reference_gpu_build_exports_its_symbols():
+    """The reference's CUDA path built for sm_100a (oracle/_ref, the timed
+    "plain GPU path" baseline) loads without a GPU and exports the two
+    symbols beampower/core.py:65-87 binds."""
+    import ctypes as ct
+    from oracle.oracle import REF_GPU_SO
+    if not os.path.exists(REF_GPU_SO):
+        pytest.skip("reference GPU library not built (oracle/_ref)")
+    lib = ct.CDLL(REF_GPU_SO)
+    assert hasattr(lib, "beamform") and hasattr(lib, "beamform_max")
